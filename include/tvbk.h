@@ -1,0 +1,204 @@
+/*
+ * tvbk.h -- C ABI of the B200 region-simulation kernels (libtvbk.so).
+ *
+ * The library runs TVB's region simulation loop -- delayed-history gather,
+ * coupling pre/sum/post, model derivative, Euler/Heun (deterministic and
+ * stochastic) step with additive noise, and the Raw / TemporalAverage / Bold
+ * monitors -- for a batch of independent simulation instances in one launch.
+ *
+ * Every entry point takes plain pointers and sizes.  Device buffers are
+ * allocated and owned by the caller; the library allocates nothing, except
+ * where a function's comment says otherwise.  Functions return TVBK_OK (0) or
+ * a negative status; tvbk_last_error() gives the message of the last failure
+ * on the calling thread.  Launches are asynchronous on the caller's stream
+ * (a cudaStream_t passed as void*; NULL is the legacy default stream).
+ *
+ * Which reference interface each entry point replaces (paths inside
+ * the-virtual-brain/tvb-root):
+ *   tvbk_idelays           tvb_library/tvb/datatypes/connectivity.py:275,308-326
+ *                          (Connectivity.configure delays + set_idelays)
+ *   tvbk_sparse_layout     tvb_library/tvb/simulator/history.py:221-244
+ *                          (SparseHistory.__init__ non-zero arrays)
+ *   tvbk_sim_run           tvb_library/tvb/simulator/simulator.py:322-366
+ *                          (Simulator.__call__ step loop: history.py:197-204,251-256,
+ *                          coupling.py:118-167, integrators.py:296-426, noise.py:195-232,
+ *                          monitors.py:178-190,380-391,942-962)
+ *   tvbk_gather_delayed    tvb_library/tvb/simulator/history.py:251-256
+ *                          (SparseHistory.query_sparse, the delayed-state gather alone)
+ *   tvbk_fc                tvb_framework/tvb/adapters/analyzers/cross_correlation_adapter.py:348-380
+ *                          (numpy.corrcoef over the Bold time series, per instance)
+ */
+#ifndef TVBK_H
+#define TVBK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TVBK_ABI_VERSION 1
+
+/* status codes */
+#define TVBK_OK 0
+#define TVBK_ERR_INVALID (-1)     /* bad argument */
+#define TVBK_ERR_UNSUPPORTED (-2) /* component combination not built */
+#define TVBK_ERR_CUDA (-3)        /* CUDA runtime error (message has the CUDA error string) */
+#define TVBK_ERR_TOO_LARGE (-4)   /* size beyond a documented limit */
+
+/* per-instance status bits written by the simulation kernel */
+#define TVBK_STATUS_NONFINITE 1   /* a state variable became NaN or Inf */
+
+/* components */
+enum {
+    TVBK_MODEL_G2D = 0,        /* Generic2dOscillator (models/oscillator.py:39-395) */
+    TVBK_MODEL_JANSEN_RIT = 1, /* JansenRit (models/jansen_rit.py:38-289) */
+    TVBK_MODEL_RWW = 2,        /* ReducedWongWang (models/wong_wang.py:36-181) */
+    TVBK_MODEL_EPILEPTOR = 3,  /* Epileptor (models/epileptor.py:36-356) */
+    TVBK_MODEL_SUM = 4         /* dx = x + c; the model of the reference's exact-propagation test */
+};
+enum {
+    TVBK_CFUN_LINEAR = 0,        /* Linear: a*gx + b (coupling.py:170-200) */
+    TVBK_CFUN_DIFFERENCE = 1,    /* Difference: a * sum w (x_j - x_i) (coupling.py:462-486) */
+    TVBK_CFUN_SIGMOIDAL_JR = 2   /* SigmoidalJansenRit (coupling.py:325-376) */
+};
+enum {
+    TVBK_SCHEME_EULER_DET = 0,   /* integrators.py:365-391 */
+    TVBK_SCHEME_EULER_STOCH = 1, /* integrators.py:394-426 */
+    TVBK_SCHEME_HEUN_DET = 2,    /* integrators.py:286-318 */
+    TVBK_SCHEME_HEUN_STOCH = 3,  /* integrators.py:321-362 */
+    TVBK_SCHEME_IDENTITY = 4     /* integrators.py:483-507 */
+};
+enum {
+    TVBK_NOISE_NONE = 0,
+    TVBK_NOISE_FED = 1,          /* caller-provided standard normals (e.g. the reference's own stream) */
+    TVBK_NOISE_PHILOX = 2        /* counter-based Philox4x32-10 + Box-Muller, keyed by (seed, stream) */
+};
+
+/* Maximum sizes of this build. */
+#define TVBK_MAX_REGIONS 1024    /* regions per instance (one thread per region) */
+#define TVBK_MAX_VOI 8           /* observed variables per monitor set */
+#define TVBK_MAX_PARAMS 20       /* model parameters */
+
+/* One connectome edge as the gather reads it: off = (idelay * n - col) * ncvar,
+ * so that the ring offset of the delayed value is (slot of step - 1) * n * ncvar
+ * - off, plus ring_len * n * ncvar when that is negative. */
+typedef struct tvbk_edge {
+    int32_t off;
+    float weight;
+} tvbk_edge;
+
+/*
+ * One simulation instance.  All pointers are device pointers.  Arrays
+ * indexed [..][n] are region-fastest.  The ring holds the coupling variables
+ * of time t in slot t % ring_len, laid out [ring_len][n][ncvar]; ring_len is
+ * at least horizon + 1 (see tvbk_ring_len).  Instances may share the
+ * connectome arrays.  The kernel advances `step` itself, so a chunked run
+ * re-launches the same descriptor array.
+ */
+typedef struct tvbk_inst {
+    /* connectome: rows are target regions, edges in the reference's row-major non-zero order */
+    const int32_t* row_ptr;      /* [n+1] */
+    const tvbk_edge* edges;      /* [nnz] packed offsets and weights (tvbk_pack_edges) */
+    /* dynamic state */
+    float* ring;                 /* [ring_len][n][ncvar] */
+    float* state;                /* [nsv][n] */
+    /* parameters */
+    const float* params;         /* [nparam][n] model parameters, one value per region */
+    const float* noise_sigma;    /* [nintvar][n] sqrt(dt) * sqrt(2 nsig); NULL when deterministic */
+    const float* noise_fed;      /* [*][nintvar][n] standard normals; step s reads row s - fed_base - 1 */
+    /* monitors (NULL disables one) */
+    float* raw;                  /* [*][nvoi][n]; step s writes row s - raw_base - 1 */
+    float* tavg;                 /* [*][nvoi][n]; sample s / tavg_istep - tavg_base - 1 */
+    float* tavg_acc;             /* [nvoi][n] running sum of the current period */
+    double* bold;                /* [*][nvoi][n]; sample s / bold_istep - bold_base - 1 */
+    double* bold_acc;            /* [nvoi][n] running sum of the current 4 ms window */
+    double* bold_stock;          /* [stock_len][nvoi][n] 4 ms averages, ring */
+    const double* hrf;           /* [stock_len] reversed haemodynamic kernel */
+    int64_t step;                /* last completed step (the reference's current_step) */
+    int64_t step_end;            /* run until step == step_end */
+    int64_t raw_base, fed_base, tavg_base, bold_base;
+    int32_t n, nnz, horizon, ring_len;
+    int32_t tavg_istep, bold_istep, bold_ii, stock_len;
+    float cfun[6];               /* coupling parameters, see tvbk_sim_run */
+    uint32_t seed, stream;       /* Philox key */
+    double bold_k1v0;            /* k_1 * V_0 of the FirstOrderVolterra kernel */
+} tvbk_inst;
+
+/* Launch description shared by all instances of one tvbk_sim_run call. */
+typedef struct tvbk_launch {
+    tvbk_inst* insts;            /* device array [n_inst]; the kernel advances each `step` */
+    int32_t* status;             /* device array [n_inst], TVBK_STATUS_* bits are OR-ed in */
+    int32_t n_inst;
+    int32_t model, cfun, scheme, noise;
+    int32_t nvoi;
+    int32_t voi[TVBK_MAX_VOI];   /* indices into the model's observable expressions */
+    int32_t max_n;               /* largest n over the instances (sets the block size) */
+    int32_t max_ring_len;        /* largest ring_len; the ring is staged in shared memory if it fits */
+    int32_t sync_every;          /* barrier interval K, 1 <= K <= min(d_min + 1, ring_len - horizon) */
+    int32_t ring_in_smem;        /* 1: stage rings in shared memory (needs fit), 0: read them in place */
+    int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */
+    float dt;
+} tvbk_launch;
+
+/* Library information. */
+int tvbk_abi_version(void);
+const char* tvbk_last_error(void);
+
+/* sizeof(tvbk_inst), sizeof(tvbk_launch), sizeof(tvbk_edge) for which = 0, 1, 2
+ * (lets a binding check its struct mirrors); -1 otherwise. */
+int64_t tvbk_sizeof(int32_t which);
+
+/* Conduction delays in integration steps, exactly as the reference:
+ * idelays = rint((tract_lengths / speed) / dt) in float64, round half to even;
+ * *horizon = max(idelays) + 1 over all n_elems entries.  Host function. */
+int tvbk_idelays(const double* tract_lengths, int64_t n_elems, double speed, double dt,
+                 int32_t* idelays, int32_t* horizon);
+
+/* Non-zero layout of an n x n weight matrix (row-major order of the non-zero
+ * entries, as SparseHistory builds it).  Host function.  row_ptr has n+1
+ * entries; col, idelay, weight have room for n*n entries; *nnz is set. */
+int tvbk_sparse_layout(const double* weights, const int32_t* idelays, int32_t n,
+                       int32_t* row_ptr, int32_t* col, int32_t* idelay, float* weight,
+                       int32_t* nnz, int32_t* min_delay);
+
+/* Pack CSR columns, delays and weights into gather edges for a ring with
+ * n regions and ncvar coupling variables.  Host function. */
+int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weight, int32_t nnz,
+                    int32_t n, int32_t ncvar, tvbk_edge* edges);
+
+/* Smallest ring length (slots) usable with barrier interval sync_every. */
+int32_t tvbk_ring_len(int32_t horizon, int32_t sync_every);
+
+/* Shared memory bytes one instance needs to stage its ring; 0 if it cannot be staged. */
+int64_t tvbk_ring_smem_bytes(int32_t n, int32_t ncvar, int32_t ring_len);
+
+/* Number of coupling variables, state variables, integrated state variables
+ * and observable expressions of a model. */
+int tvbk_model_dims(int32_t model, int32_t* ncvar, int32_t* nsv, int32_t* nintvar, int32_t* nobs,
+                    int32_t* nparam);
+
+/* Run up to L->max_steps steps of every instance (one CTA per instance).
+ * Coupling parameters in tvbk_inst.cfun: Linear {a, b}; Difference {a};
+ * SigmoidalJansenRit {cmin, cmax, midpoint, r, a}. */
+int tvbk_sim_run(const tvbk_launch* L, void* stream);
+
+/* Delayed-state gather of one instance at step `step` (the values the
+ * coupling of that step reads): out[e * ncvar + k] = ring value of variable k
+ * of region col[e] at time step - 1 - idelay[e], for every edge e.  Used to
+ * check the ring indexing bit-exactly against the reference; it reads the
+ * ring in place (inst_host->ring) through inst_host->edges, the same address
+ * arithmetic as the simulation kernel. */
+int tvbk_gather_delayed(const tvbk_inst* inst_host, int32_t ncvar, int64_t step, float* out_dev,
+                        void* stream);
+
+/* Pearson correlation of each instance's series: x is [n_inst][T][n] float64
+ * (instance-major), fc is [n_inst][n][n] float64.  Rows with zero variance
+ * give NaN like numpy.corrcoef. */
+int tvbk_fc(const double* x, int32_t n_inst, int32_t T, int32_t n, double* fc, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TVBK_H */

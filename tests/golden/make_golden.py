@@ -1,0 +1,489 @@
+"""Generate the golden fixtures for the region simulation loop by running the
+reference TVB library (numpy path) on seeded synthetic connectomes.
+
+This script is test infrastructure: it needs the reference source tree (the
+``tvb_library`` directory of the-virtual-brain/tvb-root) and its numpy/numba
+dependencies, and it is only run where that tree exists.  The fixtures it
+writes (``tests/golden/*.npz``) are what the tests read; nothing at test time
+imports the reference.
+
+    python tests/golden/make_golden.py --ref /root/reference/tvb_library [--only NAME ...]
+
+Every fixture records the raw inputs (weights, tract lengths, speed, dt,
+component parameters), the configured state the reference produced
+(idelays, horizon, the float32 history ring, the float64 current state and
+step) and the monitor outputs, for the stock reference (float32 history and
+weights, see ``tvb/simulator/history.py:49-51,166-172``) and, where noted, for
+an all-float64 variant obtained by switching those descriptors to float64.
+
+Stochastic fixtures store a SHA-256 of the noise the reference drew (recorded
+by wrapping ``integrator.noise.generate``) plus a flag saying that the stream
+is reproduced by ``numpy.random.RandomState(noise_seed)`` after the
+initial-condition draws (``tvb/simulator/models/base.py:138-155``,
+``tvb/simulator/noise.py:195-198``), so the tests regenerate the exact noise
+instead of storing hundreds of MB of it.
+"""
+import argparse
+import hashlib
+import logging
+import os
+import sys
+import time
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def synthetic_connectome(n, density, lo, hi, seed):
+    """Seeded synthetic connectome: symmetric lognormal(0,1) weights on a random
+    upper-triangle mask, normalised to max 1, zero diagonal; symmetric uniform
+    tract lengths with zero diagonal."""
+    rng = np.random.default_rng(seed)
+    w = rng.lognormal(0.0, 1.0, (n, n))
+    mask = np.triu(rng.random((n, n)) < density, 1)
+    w = np.triu(w * mask, 1)
+    w = w + w.T
+    w /= w.max()
+    lengths = np.triu(rng.uniform(lo, hi, (n, n)), 1)
+    lengths = lengths + lengths.T
+    return w, lengths
+
+
+def import_reference(ref):
+    sys.path.insert(0, ref)
+    warnings.filterwarnings("ignore")
+    logging.disable(logging.WARNING)
+    import tvb.simulator.simulator as simulator
+    import tvb.simulator.models as models
+    import tvb.simulator.coupling as coupling
+    import tvb.simulator.integrators as integrators
+    import tvb.simulator.monitors as monitors
+    import tvb.simulator.noise as noise
+    import tvb.simulator.history as history
+    from tvb.datatypes.connectivity import Connectivity
+    from tvb.basic.neotraits.api import List
+    return dict(simulator=simulator, models=models, coupling=coupling,
+                integrators=integrators, monitors=monitors, noise=noise,
+                history=history, Connectivity=Connectivity, List=List)
+
+
+FP64_FIELDS = {
+    'BaseHistory': ['weights', 'delays'],
+    'DenseHistory': ['es_weights', 'buffer', 'current_state', 'delayed_state'],
+    'SparseHistory': ['nnz_weights'],
+}
+
+
+def set_history_dtype(R, code):
+    """Switch the reference history descriptors between float32 ('f', stock)
+    and float64 ('d', all-FP64 variant)."""
+    for cls_name, fields in FP64_FIELDS.items():
+        cls = getattr(R['history'], cls_name)
+        for f in fields:
+            cls.__dict__[f].dtype = code
+
+
+def make_conn(R, w, lengths, speed):
+    n = w.shape[0]
+    return R['Connectivity'](weights=w, tract_lengths=lengths, speed=np.array([speed]),
+                             region_labels=np.array(['r%d' % i for i in range(n)]),
+                             centres=np.zeros((n, 3)))
+
+
+class NoiseRecorder:
+    def __init__(self, sim, keep=False):
+        self.h = hashlib.sha256()
+        self.count = 0
+        self.keep = keep
+        self.kept = []
+        noise = sim.integrator.noise
+        orig = noise.generate
+
+        def gen(shape, lo=-1.0, hi=1.0):
+            z = orig(shape, lo, hi)
+            self.h.update(np.ascontiguousarray(z, dtype=np.float64).tobytes())
+            self.count += 1
+            if self.keep:
+                self.kept.append(z.copy())
+            return z
+        noise.generate = gen
+
+
+def regen_noise_hash(seed, ic_ranges, horizon, n, nintvar, n_steps, dt, chunk=20000):
+    """Re-create the reference noise stream with RandomState(seed): first the
+    initial-history uniform draws, then one normal draw of shape
+    (nintvar, n, 1) per step scaled by sqrt(dt)."""
+    rs = np.random.RandomState(seed)
+    for lo, hi in ic_ranges:
+        rs.uniform(low=lo, high=hi, size=(horizon, n, 1))
+    h = hashlib.sha256()
+    left = n_steps
+    while left > 0:
+        k = min(chunk, left)
+        z = np.sqrt(dt) * rs.normal(size=(k, nintvar, n, 1))
+        for s in range(k):
+            h.update(np.ascontiguousarray(z[s]).tobytes())
+        left -= k
+    return h.hexdigest()
+
+
+def configured_state(sim):
+    hist = sim.history
+    return dict(
+        idelays=np.asarray(sim.connectivity.idelays, dtype=np.int32),
+        horizon=np.int64(sim.connectivity.horizon),
+        buffer0=np.array(hist.buffer[..., 0]),          # (H, ncvar, n)
+        state0=np.array(sim.current_state[..., 0]),      # (nsv, n)
+        step0=np.int64(sim.current_step),
+        nnz_row=np.asarray(hist.nnz_row_el_idx, dtype=np.int32),
+        nnz_col=np.asarray(hist.nnz_col_el_idx, dtype=np.int32),
+        nnz_w=np.array(hist.nnz_weights),
+        nnz_d=np.asarray(hist.nnz_idelays, dtype=np.int32),
+    )
+
+
+def run_sim(R, build, length, fp64, ic_seed=None, record_noise=False):
+    set_history_dtype(R, 'd' if fp64 else 'f')
+    try:
+        sim = build()
+        if ic_seed is not None:
+            np.random.seed(ic_seed)
+        sim.configure()
+        cfg = configured_state(sim)
+        rec = NoiseRecorder(sim) if record_noise else None
+        t0 = time.time()
+        out = sim.run(simulation_length=length)
+        el = time.time() - t0
+    finally:
+        set_history_dtype(R, 'f')
+    return sim, cfg, out, rec, el
+
+
+# inputs that the tests regenerate bit-exactly from their recipe (synthetic
+# connectome seed, initial-history seed, tract lengths / speed / dt) are kept
+# as SHA-256 digests once they are larger than this
+HASH_LIMIT = 300 * 1024
+HASHABLE = ('weights', 'tract_lengths', 'idelays', 'buffer0', 'buffer0_fp64',
+            'nnz_row', 'nnz_col', 'nnz_w', 'nnz_d')
+
+
+def sha256_array(a):
+    a = np.ascontiguousarray(a)
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def compact(arrays):
+    out = {}
+    for k, v in arrays.items():
+        base = k.split('_')[0] if k.startswith('buffer0_') and k[8:].isdigit() else k
+        if (k in HASHABLE or base == 'buffer0') and isinstance(v, np.ndarray) and v.nbytes > HASH_LIMIT:
+            out[k + '_sha256'] = sha256_array(v)
+            out[k + '_dtype'] = str(v.dtype)
+            out[k + '_shape'] = np.array(v.shape)
+        else:
+            out[k] = v
+    return out
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name + '.npz')
+    np.savez_compressed(path, **compact(arrays))
+    print('wrote', path, '%.1f KB' % (os.path.getsize(path) / 1024.0), flush=True)
+
+
+# --------------------------------------------------------------------------- cases
+
+def case_g2d(R):
+    """Generic2dOscillator, 76 regions, Linear a=0.0152, HeunDeterministic dt 0.1,
+    Raw + TemporalAverage(1 ms), 150 ms (1500 steps)."""
+    w, L = synthetic_connectome(76, 0.40, 10.0, 200.0, seed=1)
+    speed, dt, length = 3.0, 0.1, 150.0
+
+    def build():
+        return R['simulator'].Simulator(
+            model=R['models'].Generic2dOscillator(),
+            connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].Linear(a=np.array([0.0152])),
+            integrator=R['integrators'].HeunDeterministic(dt=dt),
+            monitors=[R['monitors'].Raw(), R['monitors'].TemporalAverage(period=1.0)],
+            simulation_length=length)
+    res = {}
+    for var in ('stock', 'fp64'):
+        sim, cfg, out, _, el = run_sim(R, build, length, var == 'fp64', ic_seed=101)
+        (tr, raw), (tt, tavg) = out
+        res[var] = dict(cfg=cfg, raw=raw[..., 0], raw_t=tr, tavg=tavg[..., 0], tavg_t=tt, el=el)
+    c = res['stock']['cfg']
+    save('g2d_76', weights=w, tract_lengths=L, speed=speed, dt=dt, length=length,
+         conn_recipe=np.array([76, 0.40, 10.0, 200.0, 1]), ic_seed=101,
+         coupling_a=0.0152, **c,
+         buffer0_fp64=res['fp64']['cfg']['buffer0'],
+         raw=res['stock']['raw'], raw_t=res['stock']['raw_t'],
+         tavg=res['stock']['tavg'], tavg_t=res['stock']['tavg_t'],
+         raw_fp64=res['fp64']['raw'], tavg_fp64=res['fp64']['tavg'],
+         ref_seconds=res['stock']['el'])
+
+
+def case_jr(R, length=4000.0):
+    """JansenRit, 192 regions, SigmoidalJansenRit, HeunStochastic dt 0.05 with
+    additive nsig 1e-5 on y4 only, TemporalAverage(1 ms) + Bold(2000 ms)."""
+    w, L = synthetic_connectome(192, 0.25, 5.0, 250.0, seed=2)
+    speed, dt = 4.0, 0.05
+    nsig = np.array([0, 0, 0, 0, 1e-5, 0.0])
+
+    def build():
+        return R['simulator'].Simulator(
+            model=R['models'].JansenRit(),
+            connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].SigmoidalJansenRit(),
+            integrator=R['integrators'].HeunStochastic(
+                dt=dt, noise=R['noise'].Additive(nsig=nsig.copy())),
+            monitors=[R['monitors'].TemporalAverage(period=1.0), R['monitors'].Bold(period=2000.0)],
+            simulation_length=length)
+    res = {}
+    for var in ('stock', 'fp64'):
+        sim, cfg, out, rec, el = run_sim(R, build, length, var == 'fp64', record_noise=True)
+        (tt, tavg), (tb, bold) = out
+        res[var] = dict(cfg=cfg, tavg=tavg[..., 0], tavg_t=tt, bold=bold[..., 0], bold_t=tb,
+                        noise_hash=rec.h.hexdigest(), noise_count=rec.count, el=el)
+        print('jr', var, el, flush=True)
+    sim_model = R['models'].JansenRit()
+    ranges = [sim_model.state_variable_range[sv] for sv in sim_model.state_variables]
+    c = res['stock']['cfg']
+    n_steps = int(np.ceil(length / dt))
+    regen = regen_noise_hash(42, ranges, int(c['horizon']), 192, 6, n_steps, dt)
+    assert regen == res['stock']['noise_hash'] == res['fp64']['noise_hash'], 'noise regen mismatch'
+    sub = slice(19, None, 20)  # every 20th TemporalAverage sample keeps the fixture small
+    save('jr_192', weights=w, tract_lengths=L, speed=speed, dt=dt, length=length, nsig=nsig,
+         conn_recipe=np.array([192, 0.25, 5.0, 250.0, 2]),
+         noise_seed=42, noise_regen_ok=True, noise_hash=res['stock']['noise_hash'], **c,
+         tavg_index=np.arange(len(res['stock']['tavg_t']))[sub],
+         tavg=res['stock']['tavg'][sub], tavg_t=res['stock']['tavg_t'][sub],
+         tavg_fp64=res['fp64']['tavg'][sub],
+         bold=res['stock']['bold'], bold_t=res['stock']['bold_t'], bold_fp64=res['fp64']['bold'],
+         ref_seconds=res['stock']['el'])
+
+
+RWW_G = np.logspace(-3, 0, 32)
+RWW_NSIG = np.logspace(-4, -2, 32)
+
+
+def case_rww(R, name, points, length, with_tavg):
+    """ReducedWongWang, 68 regions, Linear a=G, EulerStochastic dt 0.1 with
+    additive nsig, Bold(2000 ms) (+ TemporalAverage(100 ms) for short runs),
+    one reference simulation per (G, nsig) sweep point."""
+    w, L = synthetic_connectome(68, 0.30, 10.0, 200.0, seed=3)
+    speed, dt = 5.0, 0.1
+    out_arrays = {}
+    for k, (gi, si) in enumerate(points):
+        G, s = RWW_G[gi], RWW_NSIG[si]
+
+        def build():
+            mons = [R['monitors'].Bold(period=2000.0)]
+            if with_tavg:
+                mons.append(R['monitors'].TemporalAverage(period=100.0))
+            return R['simulator'].Simulator(
+                model=R['models'].ReducedWongWang(),
+                connectivity=make_conn(R, w, L, speed),
+                coupling=R['coupling'].Linear(a=np.array([G])),
+                integrator=R['integrators'].EulerStochastic(
+                    dt=dt, noise=R['noise'].Additive(nsig=np.array([s]))),
+                monitors=mons, simulation_length=length)
+        for var in ('stock', 'fp64'):
+            sim, cfg, out, rec, el = run_sim(R, build, length, var == 'fp64', record_noise=True)
+            print(name, k, var, '%.1fs' % el, flush=True)
+            tb, bold = out[0]
+            sfx = '' if var == 'stock' else '_fp64'
+            out_arrays['bold%s_%d' % (sfx, k)] = bold[..., 0]
+            if with_tavg:
+                out_arrays['tavg%s_%d' % (sfx, k)] = out[1][1][..., 0]
+                out_arrays['tavg_t'] = out[1][0]
+            out_arrays['bold_t'] = tb
+            if var == 'stock':
+                out_arrays['noise_hash_%d' % k] = rec.h.hexdigest()
+                cfg0 = cfg
+                out_arrays['buffer0_%d' % k] = cfg['buffer0']
+                out_arrays['state0_%d' % k] = cfg['state0']
+                out_arrays['ref_seconds_%d' % k] = el
+                hrf = sim.monitors[0].hemodynamic_response_function[0]
+        # FC exactly as the framework analyzer does it: corrcoef over time
+        out_arrays['fc_%d' % k] = np.corrcoef(out_arrays['bold_%d' % k][:, 0, :].T)
+        out_arrays['fc_fp64_%d' % k] = np.corrcoef(out_arrays['bold_fp64_%d' % k][:, 0, :].T)
+    ranges = [R['models'].ReducedWongWang().state_variable_range['S']]
+    n_steps = int(np.ceil(length / dt))
+    regen = regen_noise_hash(42, ranges, int(cfg0['horizon']), 68, 1, n_steps, dt)
+    for k in range(len(points)):
+        assert out_arrays['noise_hash_%d' % k] == regen, 'noise regen mismatch'
+    c = {k: v for k, v in cfg0.items() if k not in ('buffer0', 'state0')}
+    save(name, weights=w, tract_lengths=L, speed=speed, dt=dt, length=length,
+         conn_recipe=np.array([68, 0.30, 10.0, 200.0, 3]),
+         G=np.array([RWW_G[g] for g, _ in points]), nsig=np.array([RWW_NSIG[s] for _, s in points]),
+         point_index=np.array(points), noise_seed=42, noise_regen_ok=True, hrf=hrf,
+         **c, **out_arrays)
+
+
+def case_epi(R, name, n, density, length, gains, seed):
+    """Epileptor with x0 ~ U[-2.4,-1.6] per region, Difference coupling,
+    HeunDeterministic dt 0.05, TemporalAverage(1 ms)."""
+    w, L = synthetic_connectome(n, density, 5.0, 300.0, seed=seed)
+    x0 = np.random.default_rng(seed + 1000).uniform(-2.4, -1.6, n)
+    speed, dt = 3.0, 0.05
+
+    def build():
+        m = R['models'].Epileptor(x0=x0.copy(), **{k: np.array([v]) for k, v in gains.items()})
+        return R['simulator'].Simulator(
+            model=m, connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].Difference(),
+            integrator=R['integrators'].HeunDeterministic(dt=dt),
+            monitors=[R['monitors'].TemporalAverage(period=1.0)],
+            simulation_length=length)
+    res = {}
+    for var in ('stock', 'fp64'):
+        sim, cfg, out, _, el = run_sim(R, build, length, var == 'fp64', ic_seed=seed + 200)
+        print(name, var, '%.1fs' % el, flush=True)
+        (tt, tavg), = out
+        res[var] = dict(cfg=cfg, tavg=tavg[..., 0], tavg_t=tt, el=el)
+    c = res['stock']['cfg']
+    save(name, weights=w, tract_lengths=L, speed=speed, dt=dt, length=length, x0=x0,
+         conn_recipe=np.array([n, density, 5.0, 300.0, seed]), ic_seed=seed + 200,
+         gain_names=np.array(list(gains.keys())), gain_values=np.array(list(gains.values()), dtype=float),
+         **c, tavg=res['stock']['tavg'], tavg_t=res['stock']['tavg_t'],
+         tavg_fp64=res['fp64']['tavg'], ref_seconds=res['stock']['el'])
+
+
+def case_propagation(R):
+    """Exact delayed propagation on a 4-node chain: identity coupling, a model
+    whose derivative is state + coupling, the Identity integrator, dt = 1,
+    tract lengths 0..15 at speed 1 and a provided 16-step initial history of
+    ones (this also starts the loop at current_step = 15)."""
+    models, coupling = R['models'], R['coupling']
+
+    class PassThrough(coupling.SparseCoupling):
+        def pre(self, x_i, x_j):
+            return x_j
+
+        def post(self, gx):
+            return gx
+
+    class StatePlusInput(models.Model):
+        nvar = 1
+        _nvar = 1
+        state_variable_range = {'x': [0, 100]}
+        variables_of_interest = R['List'](of=str, default=('x',), choices=('x',))
+        state_variables = ('x',)
+        cvar = np.array([0])
+
+        def dfun(self, X, c, local_coupling=0):
+            return X + c + local_coupling
+
+    n = 4
+    w = np.zeros((n, n))
+    for i in range(n - 1):
+        w[i, i + 1] = 1.0
+    L = np.arange(n * n, dtype=float).reshape((n, n))
+    sim = R['simulator'].Simulator(
+        conduction_speed=1.0, coupling=PassThrough(), integrator=R['integrators'].Identity(dt=1.0),
+        initial_conditions=np.ones((n * n, 1, n, 1)), simulation_length=10.0,
+        connectivity=R['Connectivity'](region_labels=np.array(['']), weights=w, tract_lengths=L,
+                                       speed=np.array([1.0]), centres=np.array([0.0])),
+        model=StatePlusInput(), monitors=(R['monitors'].Raw(),))
+    sim.configure()
+    cfg = configured_state(sim)
+    xs = np.array([raw.flat[:].copy() for (t, raw), in sim(simulation_length=10)])
+    save('propagation_4', weights=w, tract_lengths=L, speed=1.0, dt=1.0, **cfg, raw=xs)
+
+
+def case_steady(R):
+    """Single-node fixed points reached by Model.stationary_trajectory (Euler,
+    dt 0.01, 2000 steps, zero coupling, start at the middle of each state range)."""
+    out = {}
+    for name in ('Generic2dOscillator', 'JansenRit', 'ReducedWongWang'):
+        model = getattr(R['models'], name)()
+        model.configure()
+        nv = len(model.state_variables)
+        init = np.zeros((nv, 1))
+        for i, (lo, hi) in enumerate(model.state_variable_range.values()):
+            init[i, :] = (hi + lo) / 2.0
+        t, y = model.stationary_trajectory(initial_conditions=init, n_step=2000, dt=0.01)
+        out[name + '_init'] = init[:, 0]
+        out[name + '_traj'] = y[:, :, 0, 0]
+    save('steady_state', **out)
+
+
+def case_idelays(R):
+    """Conduction delays in integration steps at and near rounding ties."""
+    rng = np.random.default_rng(7)
+    n = 24
+    L = rng.uniform(0.0, 60.0, (n, n))
+    # exact .5 ties at speed 1, dt 1 and decimal values near ties at dt 0.1 / 0.05
+    L[0, :12] = np.arange(12) + 0.5
+    L[1, :12] = (np.arange(12) + 0.5) * 0.1
+    L[2, :12] = np.round(rng.uniform(0, 30, 12), 2)
+    L[3, :12] = (np.arange(12) * 0.05 + 0.025)
+    res = {}
+    for speed in (1.0, 3.0, 4.0, 5.0):
+        for dt in (1.0, 0.1, 0.05, 0.0125):
+            c = R['Connectivity'](weights=np.ones((n, n)), tract_lengths=L, speed=np.array([speed]),
+                                  region_labels=np.array(['r%d' % i for i in range(n)]),
+                                  centres=np.zeros((n, 3)))
+            c.configure()
+            c.set_idelays(dt)
+            res['idelays_s%g_dt%g' % (speed, dt)] = np.asarray(c.idelays, dtype=np.int32)
+            res['horizon_s%g_dt%g' % (speed, dt)] = np.int64(c.horizon)
+    save('idelays', tract_lengths=L, **res)
+
+
+def case_difference(R):
+    """Difference coupling on two nodes with zero delays (state 1 and 2)."""
+    H = R['history']
+    w = np.array([[0.0, 1.0], [1.0, 0.0]])
+    hist = H.SparseHistory(w, np.zeros((2, 2), dtype=int), np.r_[0], 1)
+    hist.update(0, np.array([[[1.0], [2.0]]]))
+    k = R['coupling'].Difference()
+    k.configure()
+    res = k(0 + 1, hist)  # coupling for step 1 reads the state stored at step 0
+    lin = R['coupling'].Linear(a=np.array([0.5]), b=np.array([0.25]))
+    lin.configure()
+    res_lin = lin(1, hist)
+    save('difference_2', weights=w, state=np.array([1.0, 2.0]), difference=res[:, :, 0],
+         a=0.1, linear=res_lin[:, :, 0], linear_a=0.5, linear_b=0.25)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--ref', default='/root/reference/tvb_library')
+    ap.add_argument('--only', nargs='*')
+    ap.add_argument('--compact', nargs='*', help='re-save existing fixtures with large inputs hashed')
+    args = ap.parse_args()
+    if args.compact:
+        for path in args.compact:
+            d = dict(np.load(path, allow_pickle=False))
+            np.savez_compressed(path, **compact(d))
+            print('compacted', path, '%.1f KB' % (os.path.getsize(path) / 1024.0))
+        return
+    R = import_reference(args.ref)
+    cases = {
+        'propagation': lambda: case_propagation(R),
+        'steady': lambda: case_steady(R),
+        'idelays': lambda: case_idelays(R),
+        'difference': lambda: case_difference(R),
+        'g2d': lambda: case_g2d(R),
+        'epi': lambda: case_epi(R, 'epi_998', 998, 0.10, 60.0, {}, seed=4),
+        'epi_coupled': lambda: case_epi(R, 'epi_96_coupled', 96, 0.3, 200.0,
+                                        {'Ks': -0.2, 'Kf': 0.05, 'Kvf': 0.02}, seed=14),
+        'rww_short': lambda: case_rww(R, 'rww_68_short', [(0, 0), (10, 20), (20, 5), (31, 31)],
+                                      10000.0, True),
+        'rww_full': lambda: case_rww(R, 'rww_68_full', [(16, 16), (31, 8)], 60000.0, False),
+        'jr': lambda: case_jr(R),
+    }
+    for name, fn in cases.items():
+        if args.only and name not in args.only:
+            continue
+        t0 = time.time()
+        fn()
+        print('case', name, 'done in %.1fs' % (time.time() - t0), flush=True)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,244 @@
+// C ABI of libtvbk.so: argument checks, host-side planning helpers
+// (delays, non-zero layout, edge packing) and dispatch to the kernels.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "tvbk.h"
+#include "tvbk_models.cuh"
+
+namespace tvbk {
+int launch_g2d(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes);
+int launch_jr(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes);
+int launch_rww(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes);
+int launch_epileptor(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes);
+int launch_sum(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes);
+int64_t fc_smem_bytes(int32_t T, int32_t n);
+int fc_launch(const double* x, int32_t n_inst, int32_t T, int32_t n, double* fc, cudaStream_t stream);
+}  // namespace tvbk
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    return fail(TVBK_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+struct ModelDims {
+    int ncvar, nsv, nint, nobs, nparam;
+};
+
+bool model_dims(int model, ModelDims* d) {
+    using namespace tvbk;
+    switch (model) {
+        case TVBK_MODEL_G2D: *d = {G2D::NCV, G2D::NSV, G2D::NINT, G2D::NOBS, G2D::NP}; return true;
+        case TVBK_MODEL_JANSEN_RIT:
+            *d = {JansenRit::NCV, JansenRit::NSV, JansenRit::NINT, JansenRit::NOBS, JansenRit::NP};
+            return true;
+        case TVBK_MODEL_RWW: *d = {RWW::NCV, RWW::NSV, RWW::NINT, RWW::NOBS, RWW::NP}; return true;
+        case TVBK_MODEL_EPILEPTOR:
+            *d = {Epileptor::NCV, Epileptor::NSV, Epileptor::NINT, Epileptor::NOBS, Epileptor::NP};
+            return true;
+        case TVBK_MODEL_SUM:
+            *d = {SumModel::NCV, SumModel::NSV, SumModel::NINT, SumModel::NOBS, SumModel::NP};
+            return true;
+        default: return false;
+    }
+}
+
+constexpr int64_t kMaxSmemPerBlock = 227 * 1024;
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void gather_kernel(const tvbk_edge* __restrict__ edges, const float* __restrict__ ring, int nnz,
+                              int ncvar, int base_off, int ring_floats, float* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const int a = tvbk::gather_addr(base_off, edges[e].off, ring_floats);
+    for (int k = 0; k < ncvar; ++k) out[(size_t)e * ncvar + k] = ring[a + k];
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------- ABI
+
+extern "C" {
+
+int tvbk_abi_version(void) { return TVBK_ABI_VERSION; }
+
+int64_t tvbk_sizeof(int32_t which) {
+    switch (which) {
+        case 0: return (int64_t)sizeof(tvbk_inst);
+        case 1: return (int64_t)sizeof(tvbk_launch);
+        case 2: return (int64_t)sizeof(tvbk_edge);
+        default: return -1;
+    }
+}
+
+const char* tvbk_last_error(void) { return g_last_error.c_str(); }
+
+int tvbk_idelays(const double* tract_lengths, int64_t n_elems, double speed, double dt, int32_t* idelays,
+                 int32_t* horizon) {
+    if (!tract_lengths || !idelays || !horizon || n_elems <= 0)
+        return fail(TVBK_ERR_INVALID, "tvbk_idelays: null pointer or empty input");
+    if (!(speed > 0.0) || !(dt > 0.0)) return fail(TVBK_ERR_INVALID, "tvbk_idelays: speed and dt must be > 0");
+    int32_t mx = 0;
+    for (int64_t k = 0; k < n_elems; ++k) {
+        const double delay = tract_lengths[k] / speed;  // connectivity.py:275
+        const double steps = std::rint(delay / dt);     // connectivity.py:321, round half to even
+        if (!(steps >= 0.0) || steps > 2147483647.0)
+            return fail(TVBK_ERR_INVALID, "tvbk_idelays: delay %g steps out of range at %lld", steps, (long long)k);
+        idelays[k] = (int32_t)steps;
+        mx = idelays[k] > mx ? idelays[k] : mx;
+    }
+    *horizon = mx + 1;  // connectivity.py:323
+    return TVBK_OK;
+}
+
+int tvbk_sparse_layout(const double* weights, const int32_t* idelays, int32_t n, int32_t* row_ptr, int32_t* col,
+                       int32_t* idelay, float* weight, int32_t* nnz, int32_t* min_delay) {
+    if (!weights || !idelays || !row_ptr || !col || !idelay || !weight || !nnz || n <= 0)
+        return fail(TVBK_ERR_INVALID, "tvbk_sparse_layout: null pointer or n <= 0");
+    int32_t e = 0, dmin = 2147483647;
+    for (int32_t i = 0; i < n; ++i) {
+        row_ptr[i] = e;
+        for (int32_t j = 0; j < n; ++j) {
+            const double w = weights[(int64_t)i * n + j];
+            if (w != 0.0) {  // history.py:224 (mask on the float64 weights)
+                col[e] = j;
+                idelay[e] = idelays[(int64_t)i * n + j];
+                weight[e] = (float)w;  // stored float32, history.py:171,225
+                dmin = idelay[e] < dmin ? idelay[e] : dmin;
+                ++e;
+            }
+        }
+    }
+    row_ptr[n] = e;
+    *nnz = e;
+    if (min_delay) *min_delay = e > 0 ? dmin : 0;
+    return TVBK_OK;
+}
+
+int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weight, int32_t nnz, int32_t n,
+                    int32_t ncvar, tvbk_edge* edges) {
+    if ((nnz > 0 && (!col || !idelay || !weight || !edges)) || n <= 0 || ncvar <= 0)
+        return fail(TVBK_ERR_INVALID, "tvbk_pack_edges: bad arguments");
+    for (int32_t e = 0; e < nnz; ++e) {
+        if (col[e] < 0 || col[e] >= n || idelay[e] < 0)
+            return fail(TVBK_ERR_INVALID, "tvbk_pack_edges: edge %d out of range", e);
+        const int64_t off = ((int64_t)idelay[e] * n - col[e]) * ncvar;
+        if (off > 2147483647LL) return fail(TVBK_ERR_TOO_LARGE, "tvbk_pack_edges: ring offset overflows int32");
+        edges[e].off = (int32_t)off;
+        edges[e].weight = weight[e];
+    }
+    return TVBK_OK;
+}
+
+int32_t tvbk_ring_len(int32_t horizon, int32_t sync_every) {
+    if (horizon < 1 || sync_every < 1) return -1;
+    return horizon + sync_every;
+}
+
+int64_t tvbk_ring_smem_bytes(int32_t n, int32_t ncvar, int32_t ring_len) {
+    const int64_t b = (int64_t)ring_len * n * ncvar * (int64_t)sizeof(float);
+    return b <= kMaxSmemPerBlock ? b : 0;
+}
+
+int tvbk_model_dims(int32_t model, int32_t* ncvar, int32_t* nsv, int32_t* nintvar, int32_t* nobs,
+                    int32_t* nparam) {
+    ModelDims d;
+    if (!model_dims(model, &d)) return fail(TVBK_ERR_INVALID, "tvbk_model_dims: unknown model %d", model);
+    if (ncvar) *ncvar = d.ncvar;
+    if (nsv) *nsv = d.nsv;
+    if (nintvar) *nintvar = d.nint;
+    if (nobs) *nobs = d.nobs;
+    if (nparam) *nparam = d.nparam;
+    return TVBK_OK;
+}
+
+int tvbk_sim_run(const tvbk_launch* L, void* stream) {
+    if (!L) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: null launch");
+    ModelDims d;
+    if (!model_dims(L->model, &d)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: unknown model %d", L->model);
+    if (!L->insts || !L->status || L->n_inst <= 0)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: need instances and a status array");
+    if (L->n_inst > 2147483647 / 2) return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: too many instances");
+    if (L->max_n <= 0 || L->max_n > TVBK_MAX_REGIONS)
+        return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: %d regions, this build handles 1..%d", L->max_n,
+                    TVBK_MAX_REGIONS);
+    if (L->nvoi < 0 || L->nvoi > TVBK_MAX_VOI || L->nvoi > d.nobs)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: nvoi %d out of 0..%d", L->nvoi,
+                    d.nobs < TVBK_MAX_VOI ? d.nobs : TVBK_MAX_VOI);
+    for (int v = 0; v < L->nvoi; ++v)
+        if (L->voi[v] < 0 || L->voi[v] >= d.nobs)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: voi %d out of range", L->voi[v]);
+    if (L->sync_every < 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: sync_every must be >= 1");
+    if (L->max_steps < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_steps < 0");
+    if (!(L->dt > 0.0f)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: dt must be > 0");
+    const bool stoch = L->scheme == TVBK_SCHEME_EULER_STOCH || L->scheme == TVBK_SCHEME_HEUN_STOCH;
+    if (stoch && L->noise != TVBK_NOISE_FED && L->noise != TVBK_NOISE_PHILOX)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: stochastic scheme needs fed or Philox noise");
+    if (L->max_steps == 0) return TVBK_OK;
+    size_t smem = 0;
+    if (L->ring_in_smem) {
+        if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
+        const int64_t b = (int64_t)L->max_ring_len * L->max_n * d.ncvar * (int64_t)sizeof(float);
+        if (b > kMaxSmemPerBlock || L->max_n > 256)
+            return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: ring of %lld bytes / %d regions cannot be staged in "
+                        "shared memory", (long long)b, L->max_n);
+        smem = (size_t)b;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    switch (L->model) {
+        case TVBK_MODEL_G2D: rc = tvbk::launch_g2d(*L, st, smem); break;
+        case TVBK_MODEL_JANSEN_RIT: rc = tvbk::launch_jr(*L, st, smem); break;
+        case TVBK_MODEL_RWW: rc = tvbk::launch_rww(*L, st, smem); break;
+        case TVBK_MODEL_EPILEPTOR: rc = tvbk::launch_epileptor(*L, st, smem); break;
+        default: rc = tvbk::launch_sum(*L, st, smem); break;
+    }
+    if (rc == -1) return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: instance too large for this kernel variant");
+    if (rc == -2)
+        return fail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run: model %d / coupling %d / scheme %d not built", L->model,
+                    L->cfun, L->scheme);
+    if (rc != 0) return cuda_fail((cudaError_t)rc, "tvbk_sim_run launch");
+    return TVBK_OK;
+}
+
+int tvbk_gather_delayed(const tvbk_inst* I, int32_t ncvar, int64_t step, float* out_dev, void* stream) {
+    if (!I || !out_dev || !I->ring || !I->edges || ncvar < 1 || ncvar > 2)
+        return fail(TVBK_ERR_INVALID, "tvbk_gather_delayed: bad arguments");
+    if (I->nnz <= 0) return TVBK_OK;
+    const int ring_floats = I->ring_len * I->n * ncvar;
+    int64_t slot = (step - 1) % I->ring_len;
+    if (slot < 0) slot += I->ring_len;
+    const int base_off = (int)slot * I->n * ncvar;
+    const int threads = 256, blocks = (I->nnz + threads - 1) / threads;
+    gather_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(I->edges, I->ring, I->nnz, ncvar, base_off,
+                                                                 ring_floats, out_dev);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TVBK_OK : cuda_fail(e, "tvbk_gather_delayed");
+}
+
+int tvbk_fc(const double* x, int32_t n_inst, int32_t T, int32_t n, double* fc, void* stream) {
+    if (!x || !fc || n_inst <= 0 || T < 2 || n < 1) return fail(TVBK_ERR_INVALID, "tvbk_fc: bad arguments");
+    if (tvbk::fc_smem_bytes(T, n) == 0)
+        return fail(TVBK_ERR_TOO_LARGE, "tvbk_fc: series of %d x %d does not fit the shared-memory kernel", T, n);
+    const int rc = tvbk::fc_launch(x, n_inst, T, n, fc, (cudaStream_t)stream);
+    return rc == 0 ? TVBK_OK : cuda_fail((cudaError_t)rc, "tvbk_fc");
+}
+
+}  // extern "C"

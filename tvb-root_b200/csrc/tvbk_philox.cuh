@@ -1,0 +1,72 @@
+// Counter-based normal variates for the stochastic integrators.
+//
+// Philox4x32 with 10 rounds (J. K. Salmon, M. A. Moraes, R. O. Dror,
+// D. E. Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11), written
+// from the paper's round function and published multiplier / Weyl constants.
+// Uniforms are ((x >> 9) + 0.5) * 2^-23, exact in float32 and never 0 or 1;
+// a Box-Muller transform turns each pair into two normals.
+//
+// Stream layout (mirrored by the CPU oracle): the normal of (step s, region i,
+// state variable k) is element s & 3 of the 4 normals from
+// Philox(key = (seed, stream), counter = (s >> 2, i, k, 0)), the pairs
+// (x0, x1) and (x2, x3) giving steps 4q..4q+1 and 4q+2..4q+3.  The stream is
+// keyed by instance, not by batch slot, so a simulation draws the same noise
+// alone or batched with others.
+#pragma once
+#include <cstdint>
+
+namespace tvbk {
+
+struct Philox4 {
+    uint32_t x[4];
+};
+
+__device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                 uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
+        const uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+        const uint32_t n0 = hi1 ^ c1 ^ k0;
+        const uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += W0;
+        k1 += W1;
+    }
+    Philox4 out;
+    out.x[0] = c0;
+    out.x[1] = c1;
+    out.x[2] = c2;
+    out.x[3] = c3;
+    return out;
+}
+
+__device__ __forceinline__ float uniform_open(uint32_t x) {
+    return (__uint2float_rn(x >> 9) + 0.5f) * 1.1920928955078125e-07f;  // 2^-23
+}
+
+// Box-Muller: r = sqrt(-2 ln u1); (r cos 2 pi u2, r sin 2 pi u2).
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
+    const float u1 = uniform_open(a);
+    const float u2 = uniform_open(b);
+    const float r = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    z0 = r * c;
+    z1 = r * s;
+}
+
+// The 4 normals of block (s >> 2) for region i, state variable k.
+__device__ __forceinline__ void philox_normals4(uint32_t seed, uint32_t stream, int64_t step, int i, int k,
+                                                float z[4]) {
+    const Philox4 r = philox4x32_10((uint32_t)(step >> 2), (uint32_t)i, (uint32_t)k, 0u, seed, stream);
+    box_muller(r.x[0], r.x[1], z[0], z[1]);
+    box_muller(r.x[2], r.x[3], z[2], z[3]);
+}
+
+}  // namespace tvbk

@@ -1,0 +1,410 @@
+"""Device execution of a batch of simulation instances.
+
+A ``Batch`` packs every per-instance array (ring, state, parameters, noise
+scales, monitor accumulators and outputs) and the shared connectomes into
+device arenas owned by torch, writes one ``tvbk_inst`` descriptor per
+instance, and advances all instances with ``tvbk_sim_run`` in chunks.  All
+instances of a batch share model, coupling, scheme, noise kind, dt and the
+observed variables; they may differ in connectome, size, parameters,
+length and monitors' presence.
+
+Inputs travel in one host-to-device copy of a staging arena; accumulators and
+outputs are zero-filled on the device.  Outputs come back in one
+device-to-host copy.
+"""
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+
+ALIGN = 256
+
+
+def _aligned(x):
+    return (x + ALIGN - 1) // ALIGN * ALIGN
+
+
+class _Arena:
+    """Byte offsets of named regions in one allocation."""
+
+    def __init__(self):
+        self.size = 0
+        self.regions = {}
+
+    def add(self, key, nbytes):
+        off = _aligned(self.size)
+        self.regions[key] = (off, int(nbytes))
+        self.size = off + int(nbytes)
+        return off
+
+
+def ring_from_reference(buffer, step, ring_len):
+    """Reference history buffer (H, ncvar, n), time t in slot t % H for
+    t in [step - H + 1, step], to the device ring (ring_len, n, ncvar) with
+    time t in slot t % ring_len (tvb/simulator/history.py:197-204)."""
+    buf = np.asarray(buffer)
+    H, ncv, n = buf.shape
+    ring = np.zeros((ring_len, n, ncv), dtype=np.float32)
+    ts = np.arange(step - H + 1, step + 1)
+    ring[ts % ring_len] = buf[ts % H].transpose(0, 2, 1)
+    return ring
+
+
+def ring_to_reference(ring, step, horizon):
+    """Inverse of ring_from_reference for the times [step - horizon + 1, step]."""
+    ring = np.asarray(ring)
+    RL, n, ncv = ring.shape
+    out = np.zeros((horizon, ncv, n), dtype=ring.dtype)
+    ts = np.arange(step - horizon + 1, step + 1)
+    out[ts % horizon] = ring[ts % RL].transpose(0, 2, 1)
+    return out
+
+
+class Connectome:
+    """Host CSR + packed gather edges of one weight / delay matrix pair."""
+
+    def __init__(self, weights, idelays, ncvar):
+        self.row_ptr, self.col, self.idelay, self.weight, self.nnz, self.min_delay = \
+            _lib.sparse_layout(weights, idelays)
+        self.n = int(np.asarray(weights).shape[0])
+        self.horizon = int(np.asarray(idelays).max()) + 1
+        self.ncvar = ncvar
+        self.edges = _lib.pack_edges(self.col, self.idelay, self.weight, self.n, ncvar)
+
+
+class InstanceSpec:
+    """One simulation instance.
+
+    ring0: (H, ncvar, n) history as the reference lays it out, valid at step0;
+    state0: (nsv, n); params: (nparam, n) float32; cfun: coupling parameters;
+    sigma: (nintvar, n) sqrt(dt) sqrt(2 nsig) or None; n_steps: steps to run;
+    raw: keep every step; tavg_istep / bold (dict istep, ii, hrf, k1v0): monitors.
+    noise_fed: (n_steps, nintvar, n) standard normals or None.
+    """
+
+    def __init__(self, conn, ring0, state0, params, cfun, n_steps, step0=0, sigma=None, noise_fed=None,
+                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None):
+        self.conn = conn
+        self.ring0 = ring0
+        self.state0 = state0
+        self.params = params
+        self.cfun = cfun
+        self.n_steps = int(n_steps)
+        self.step0 = int(step0)
+        self.sigma = sigma
+        self.noise_fed = noise_fed
+        self.seed = int(seed)
+        self.stream = int(stream)
+        self.raw = raw
+        self.tavg_istep = int(tavg_istep)
+        self.bold = bold
+        # monitor accumulators carried over from a previous run of the same
+        # simulation: dict with 'tavg_acc' (nvoi, n), 'bold_acc' (nvoi, n),
+        # 'bold_stock' (stock_len, nvoi, n); None starts them at zero
+        self.acc0 = None
+
+
+class Batch:
+    def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
+                 sync_every=None, ring_in_smem=None):
+        self.lib = _lib.load()
+        self.device = torch.device(device if device is not None else 'cuda')
+        self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
+        self.dt = float(dt)
+        self.voi = list(voi_codes)
+        self.nvoi = len(self.voi)
+        self.specs = list(specs)
+        self.ncvar, self.nsv, self.nint, self.nobs, self.nparam = _lib.model_dims(model_id)
+        if not self.specs:
+            raise ValueError('empty batch')
+        # barrier interval: no read of a time written inside a window (K <= d_min + 1)
+        dmin = min(s.conn.min_delay for s in self.specs)
+        K = dmin + 1 if sync_every is None else int(sync_every)
+        K = max(1, min(K, dmin + 1))
+        self.max_n = max(s.conn.n for s in self.specs)
+        if self.max_n > _lib.MAX_REGIONS:
+            raise ValueError('%d regions exceed this build (%d)' % (self.max_n, _lib.MAX_REGIONS))
+        hmax = max(s.conn.horizon for s in self.specs)
+        # stage rings in shared memory when the largest fits, shrinking K if that makes it fit
+        smem_ok = self.max_n <= 256
+        if ring_in_smem is None:
+            ring_in_smem = smem_ok
+        if ring_in_smem:
+            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar, hmax + K) == 0:
+                K -= 1
+            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar, hmax + K) == 0:
+                ring_in_smem = False
+        self.sync_every = K
+        self.ring_in_smem = bool(ring_in_smem)
+        self._build()
+
+    # ------------------------------------------------------------------ build
+    def _build(self):
+        specs, nvoi = self.specs, self.nvoi
+        init, zero = _Arena(), _Arena()
+        conns = {}
+        for s in specs:
+            if id(s.conn) not in conns:
+                c = s.conn
+                conns[id(s.conn)] = c
+                init.add(('row_ptr', id(c)), c.row_ptr.nbytes)
+                init.add(('edges', id(c)), max(c.edges.nbytes, 8))
+        hrfs = {}
+        self.meta = []
+        for k, s in enumerate(specs):
+            n = s.conn.n
+            RL = s.conn.horizon + self.sync_every
+            m = dict(n=n, ring_len=RL)
+            init.add(('ring', k), RL * n * self.ncvar * 4)
+            init.add(('state', k), self.nsv * n * 4)
+            init.add(('params', k), max(self.nparam, 1) * n * 4)
+            if s.sigma is not None:
+                init.add(('sigma', k), self.nint * n * 4)
+            acc_arena = init if s.acc0 is not None else zero
+            if s.bold is not None:
+                h = s.bold['hrf']
+                if id(h) not in hrfs:
+                    hrfs[id(h)] = h
+                    init.add(('hrf', id(h)), h.nbytes)
+                acc_arena.add(('bold_acc', k), nvoi * n * 8)
+                acc_arena.add(('bold_stock', k), len(h) * nvoi * n * 8)
+            if s.tavg_istep:
+                acc_arena.add(('tavg_acc', k), nvoi * n * 4)
+            # outputs
+            s1 = s.step0 + s.n_steps
+            if s.raw:
+                m['raw_rows'] = s.n_steps
+                zero.add(('raw', k), s.n_steps * nvoi * n * 4)
+            if s.tavg_istep:
+                m['tavg_rows'] = s1 // s.tavg_istep - s.step0 // s.tavg_istep
+                zero.add(('tavg', k), max(m['tavg_rows'], 1) * nvoi * n * 4)
+            if s.bold is not None:
+                bi = s.bold['istep']
+                m['bold_rows'] = s1 // bi - s.step0 // bi
+                zero.add(('bold', k), max(m['bold_rows'], 1) * nvoi * n * 8)
+            self.meta.append(m)
+        init.add(('insts',), len(specs) * _lib.INST_DTYPE.itemsize)
+        zero.add(('status',), len(specs) * 4)
+
+        dev = self.device
+        self.init_buf = torch.empty(max(init.size, 1), dtype=torch.uint8, device=dev)
+        self.zero_buf = torch.zeros(max(zero.size, 1), dtype=torch.uint8, device=dev)
+        ib, zb = self.init_buf.data_ptr(), self.zero_buf.data_ptr()
+        self.init, self.zero = init, zero
+
+        stage = np.zeros(max(init.size, 1), dtype=np.uint8)
+
+        def put(key, arr):
+            off, nb = init.regions[key]
+            a = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
+            stage[off:off + a.size] = a
+            return ib + off
+
+        def zaddr(key):
+            if key in zero.regions:
+                return zb + zero.regions[key][0]
+            if key in init.regions:
+                return ib + init.regions[key][0]
+            return 0
+
+        cptr = {}
+        for key, c in conns.items():
+            cptr[key] = (put(('row_ptr', key), c.row_ptr), put(('edges', key), c.edges)
+                         if c.nnz else ib + init.regions[('edges', key)][0])
+        hptr = {key: put(('hrf', key), np.asarray(h, dtype=np.float64)) for key, h in hrfs.items()}
+
+        insts = np.zeros(len(specs), dtype=_lib.INST_DTYPE)
+        self._fed = []
+        for k, s in enumerate(specs):
+            m = self.meta[k]
+            n, RL = m['n'], m['ring_len']
+            d = insts[k]
+            d['row_ptr'], d['edges'] = cptr[id(s.conn)]
+            ring = ring_from_reference(s.ring0, s.step0, RL)
+            d['ring'] = put(('ring', k), ring)
+            d['state'] = put(('state', k), np.asarray(s.state0, dtype=np.float32))
+            params = np.asarray(s.params, dtype=np.float32)
+            if params.size == 0:
+                params = np.zeros((1, n), dtype=np.float32)
+            d['params'] = put(('params', k), params)
+            d['noise_sigma'] = put(('sigma', k), np.asarray(s.sigma, dtype=np.float32)) if s.sigma is not None else 0
+            if s.noise_fed is not None:
+                fed = s.noise_fed
+                if not isinstance(fed, torch.Tensor):
+                    fed = torch.from_numpy(np.ascontiguousarray(fed, dtype=np.float32))
+                fed = fed.to(dev, dtype=torch.float32).contiguous()
+                self._fed.append(fed)
+                d['noise_fed'] = fed.data_ptr()
+            if s.acc0 is not None:
+                for key, dtype in (('tavg_acc', np.float32), ('bold_acc', np.float64), ('bold_stock', np.float64)):
+                    if (key, k) in init.regions and s.acc0.get(key) is not None:
+                        put((key, k), np.asarray(s.acc0[key], dtype=dtype))
+            d['raw'] = zaddr(('raw', k))
+            d['tavg'] = zaddr(('tavg', k))
+            d['tavg_acc'] = zaddr(('tavg_acc', k))
+            d['bold'] = zaddr(('bold', k))
+            d['bold_acc'] = zaddr(('bold_acc', k))
+            d['bold_stock'] = zaddr(('bold_stock', k))
+            d['step'] = s.step0
+            d['step_end'] = s.step0 + s.n_steps
+            d['raw_base'] = s.step0
+            d['fed_base'] = s.step0
+            d['n'], d['nnz'], d['horizon'], d['ring_len'] = n, s.conn.nnz, s.conn.horizon, RL
+            if s.tavg_istep:
+                d['tavg_istep'] = s.tavg_istep
+                d['tavg_base'] = s.step0 // s.tavg_istep
+            if s.bold is not None:
+                d['hrf'] = hptr[id(s.bold['hrf'])]
+                d['bold_istep'] = s.bold['istep']
+                d['bold_ii'] = s.bold['ii']
+                d['stock_len'] = len(s.bold['hrf'])
+                d['bold_base'] = s.step0 // s.bold['istep']
+                d['bold_k1v0'] = s.bold['k1v0']
+            cf = list(s.cfun) + [0.0] * (6 - len(s.cfun))
+            d['cfun'] = cf
+            d['seed'] = s.seed & 0xFFFFFFFF
+            d['stream'] = s.stream & 0xFFFFFFFF
+        self.insts_host = insts
+        self.insts_ptr = put(('insts',), insts)
+        self.status_ptr = zaddr(('status',))
+        self.init_buf.copy_(torch.from_numpy(stage))
+        self.steps_done = 0
+        self.max_total = max(s.n_steps for s in specs)
+
+    # -------------------------------------------------------------------- run
+    def launch_struct(self, max_steps):
+        L = _lib.Launch()
+        L.insts = self.insts_ptr
+        L.status = self.status_ptr
+        L.n_inst = len(self.specs)
+        L.model, L.cfun, L.scheme, L.noise = self.model_id, self.cfun_id, self.scheme_id, self.noise_kind
+        L.nvoi = self.nvoi
+        for v, code in enumerate(self.voi):
+            L.voi[v] = code
+        L.max_n = self.max_n
+        L.max_ring_len = max(m['ring_len'] for m in self.meta)
+        L.sync_every = self.sync_every
+        L.ring_in_smem = 1 if self.ring_in_smem else 0
+        L.max_steps = int(max_steps)
+        L.dt = self.dt
+        return L
+
+    def run(self, n_steps=None, chunk=None, stream=None):
+        """Advance every instance by up to n_steps (default: to its end) in
+        launches of at most `chunk` steps."""
+        left = self.max_total - self.steps_done if n_steps is None else int(n_steps)
+        chunk = left if chunk is None else int(chunk)
+        st = torch.cuda.current_stream(self.device) if stream is None else stream
+        while left > 0:
+            k = min(chunk, left)
+            L = self.launch_struct(k)
+            _lib.check(self.lib.tvbk_sim_run(ctypes.byref(L), ctypes.c_void_p(st.cuda_stream)))
+            left -= k
+            self.steps_done += k
+
+    # ---------------------------------------------------------------- outputs
+    def _zview(self, key, dtype, shape):
+        off, nb = self.zero.regions[key]
+        t = self.zero_buf[off:off + nb].view(dtype)
+        return t[:int(np.prod(shape))].view(*shape)
+
+    def _iview(self, key, dtype, shape):
+        off, nb = self.init.regions[key]
+        t = self.init_buf[off:off + nb].view(dtype)
+        return t[:int(np.prod(shape))].view(*shape)
+
+    def outputs_device(self, k):
+        """Device tensors of instance k's outputs: raw (T, nvoi, n) f32,
+        tavg (T, nvoi, n) f32, bold (T, nvoi, n) f64."""
+        m, nvoi = self.meta[k], self.nvoi
+        out = {}
+        if 'raw_rows' in m:
+            out['raw'] = self._zview(('raw', k), torch.float32, (m['raw_rows'], nvoi, m['n']))
+        if 'tavg_rows' in m:
+            out['tavg'] = self._zview(('tavg', k), torch.float32, (m['tavg_rows'], nvoi, m['n']))
+        if 'bold_rows' in m:
+            out['bold'] = self._zview(('bold', k), torch.float64, (m['bold_rows'], nvoi, m['n']))
+        return out
+
+    def outputs_host(self):
+        """All outputs of all instances as numpy arrays, from one device-to-host copy."""
+        host = self.zero_buf.cpu().numpy()
+        res = []
+        for k, m in enumerate(self.meta):
+            o = {}
+            nvoi, n = self.nvoi, m['n']
+            for key, dt, rows in (('raw', np.float32, 'raw_rows'), ('tavg', np.float32, 'tavg_rows'),
+                                  ('bold', np.float64, 'bold_rows')):
+                if rows in m:
+                    off, nb = self.zero.regions[(key, k)]
+                    cnt = m[rows] * nvoi * n
+                    o[key] = host[off:off + nb].view(dt)[:cnt].reshape(m[rows], nvoi, n)
+            res.append(o)
+        return res
+
+    def _region_view(self, key, dtype, shape):
+        if key in self.zero.regions:
+            return self._zview(key, dtype, shape)
+        return self._iview(key, dtype, shape)
+
+    def accumulators(self, k):
+        """Monitor accumulators of instance k (to continue the simulation later)."""
+        m, nvoi, s = self.meta[k], self.nvoi, self.specs[k]
+        acc = {}
+        if ('tavg_acc', k) in self.zero.regions or ('tavg_acc', k) in self.init.regions:
+            acc['tavg_acc'] = self._region_view(('tavg_acc', k), torch.float32, (nvoi, m['n'])).cpu().numpy()
+        if s.bold is not None:
+            acc['bold_acc'] = self._region_view(('bold_acc', k), torch.float64, (nvoi, m['n'])).cpu().numpy()
+            acc['bold_stock'] = self._region_view(('bold_stock', k), torch.float64,
+                                                  (len(s.bold['hrf']), nvoi, m['n'])).cpu().numpy()
+        return acc
+
+    def status(self):
+        return self._zview(('status',), torch.int32, (len(self.specs),)).cpu().numpy()
+
+    def state(self, k):
+        return self._iview(('state', k), torch.float32, (self.nsv, self.meta[k]['n'])).cpu().numpy()
+
+    def ring(self, k):
+        m = self.meta[k]
+        return self._iview(('ring', k), torch.float32, (m['ring_len'], m['n'], self.ncvar)).cpu().numpy()
+
+    def current_step(self, k):
+        off, _ = self.init.regions[('insts',)]
+        raw = self.init_buf[off:off + len(self.specs) * _lib.INST_DTYPE.itemsize].cpu().numpy()
+        return int(raw.view(_lib.INST_DTYPE)[k]['step'])
+
+    def gather_delayed(self, k, step):
+        """Delayed values the coupling of `step` reads for every edge of instance k
+        (read through the same address arithmetic as the kernel)."""
+        m = self.meta[k]
+        conn = self.specs[k].conn
+        out = torch.empty(max(conn.nnz, 1) * self.ncvar, dtype=torch.float32, device=self.device)
+        inst = _lib.Inst()
+        d = self.insts_host[k]
+        inst.edges = int(d['edges'])
+        inst.ring = int(d['ring'])
+        inst.n, inst.nnz, inst.horizon, inst.ring_len = m['n'], conn.nnz, conn.horizon, m['ring_len']
+        st = torch.cuda.current_stream(self.device)
+        _lib.check(self.lib.tvbk_gather_delayed(ctypes.byref(inst), self.ncvar, int(step),
+                                                ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+        return out[:conn.nnz * self.ncvar].view(conn.nnz, self.ncvar).cpu().numpy()
+
+
+def functional_connectivity(series, stream=None):
+    """Pearson FC per instance on the device: series (I, T, n) float64 tensor or
+    array -> (I, n, n) float64 tensor (numpy.corrcoef over time)."""
+    lib = _lib.load()
+    x = series if isinstance(series, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(series))
+    x = x.to('cuda', dtype=torch.float64).contiguous()
+    if x.dim() == 2:
+        x = x[None]
+    I, T, n = x.shape
+    fc = torch.empty((I, n, n), dtype=torch.float64, device=x.device)
+    st = torch.cuda.current_stream(x.device) if stream is None else stream
+    _lib.check(lib.tvbk_fc(ctypes.c_void_p(x.data_ptr()), I, T, n, ctypes.c_void_p(fc.data_ptr()),
+                           ctypes.c_void_p(st.cuda_stream)))
+    return fc
