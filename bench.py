@@ -1,0 +1,312 @@
+#!/usr/bin/env python
+"""Benchmark of the batched region simulation loop on B200.
+
+Workload (one bench step): the ReducedWongWang parameter sweep -- 68-region
+seeded synthetic connectome (30 % density, tract lengths 10-200 mm, speed
+5 mm/ms), Linear coupling with G over 32 log-spaced values in [0.001, 1] x
+additive noise nsig over 32 log-spaced values in [1e-4, 1e-2] = 1024
+instances, EulerStochastic dt 0.1 ms, 60 s each (600 000 steps), Bold
+(TR 2000 ms, float64 accumulation) and per-instance FC on the device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line.  `value` is region-steps/s of the device path with the
+inputs resident in HBM (kernel launches of the sweep + FC, CUDA events);
+`e2e` is the same metric through the public ParameterSweep API from host
+arrays to host results, transfers included.  Under torchrun each rank runs
+its own 1024-instance shard (weak scaling, no collective on the data path)
+and the time is the max over ranks.  `--impl reference` times the CPU oracle
+(a numpy restatement of the reference's numpy path) on the host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.join(HERE, 'tvb-root_b200'))
+
+import numpy as np  # noqa: E402
+
+METRIC = 'region-steps/sec batched FP32 vs plain, err vs FP64 oracle; p50/p99 sim latency'
+UNIT = 'region-steps/s'
+N_REGIONS, DENSITY, L_LO, L_HI, SPEED, SEED = 68, 0.30, 10.0, 200.0, 5.0, 3
+DT = 0.1
+
+
+def sweep_grid():
+    G = np.logspace(-3, 0, 32)
+    S = np.logspace(-4, -2, 32)
+    gg, ss = np.meshgrid(G, S, indexing='ij')
+    return gg.reshape(-1), ss.reshape(-1)
+
+
+def make_sweep(instances, length_ms, rank=0, chunk=None):
+    from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.sweep import ParameterSweep
+    w, L = synthetic.connectome(N_REGIONS, DENSITY, L_LO, L_HI, seed=SEED)
+    G, S = sweep_grid()
+    idx = (np.arange(instances) + rank * instances) % G.size
+    sw = ParameterSweep(model=models.ReducedWongWang(), connectivity=Connectivity(w, L, speed=SPEED),
+                        coupling=coupling.Linear(), monitors=[monitors.Bold(period=2000.0)],
+                        integrator=integrators.EulerStochastic(dt=DT, noise=noise.Additive(nsig=[1e-3])),
+                        simulation_length=length_ms, sweep={'coupling.a': G[idx], 'noise.nsig': S[idx]},
+                        chunk_steps=chunk)
+    return sw
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+              'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+              'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith('active'):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': float(max(mx)), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+# -------------------------------------------------------------- CPU oracle
+
+def _oracle_worker(args):
+    """One reference-equivalent instance on the CPU oracle (numpy), including
+    its per-step normal draws like the reference's RandomState path."""
+    k, n_steps, G, nsig = args
+    os.environ['OMP_NUM_THREADS'] = '1'
+    from oracle import tvb_oracle as O
+    from tvb_b200 import synthetic
+    w, L = synthetic.connectome(N_REGIONS, DENSITY, L_LO, L_HI, seed=SEED)
+    idl, H = O.integer_delays(L, SPEED, DT)
+    info = O.MODEL_INFO['ReducedWongWang']
+    rs = np.random.RandomState(42)
+    hist = O.reference_initial_history(rs, [info['ranges']['S']], H, N_REGIONS)
+    t0 = time.perf_counter()
+    z = rs.normal(size=(n_steps, 1, N_REGIONS))
+    O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic', n_steps,
+               [O.Monitor('Bold', 2000.0)], hist[:, [0]].astype(np.float32), hist[0], 0, nsig=[nsig], noise_z=z)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(n_steps=20000, cores=None):
+    import multiprocessing as mp
+    cores = cores or os.cpu_count() or 1
+    G, S = sweep_grid()
+    pick = np.linspace(0, G.size - 1, cores).astype(int)
+    ctx = mp.get_context('spawn')
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        times = pool.map(_oracle_worker, [(k, n_steps, G[i], S[i]) for k, i in enumerate(pick)])
+    wall = time.perf_counter() - t0
+    rs = cores * n_steps * N_REGIONS
+    return {'value': rs / max(times), 'unit': UNIT, 'cores': cores, 'kind': 'port',
+            'sample': '%d RWW sweep instances (one per core), %d steps (%g ms) each, oracle numpy path '
+                      'incl. per-step noise draws; value = instances x steps x regions / slowest instance'
+                      % (cores, n_steps, n_steps * DT), 'wall_s': wall}
+
+
+# --------------------------------------------------------------------- main
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(n_steps=args.cpu_steps)
+    ms = 1e3 * cb['cores'] * args.cpu_steps * N_REGIONS / cb['value']
+    line = {'metric': METRIC, 'value': cb['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
+            'config': {'workload': 'rww_sweep_68r_1024i_60s_bold_fc', 'sample_only': True},
+            'cpu_baseline': cb, 'e2e': {'value': cb['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                                        'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--instances', type=int, default=1024)
+    ap.add_argument('--length', type=float, default=60000.0, help='simulated ms per instance')
+    ap.add_argument('--chunk', type=int, default=None, help='steps per kernel launch')
+    ap.add_argument('--cpu-steps', type=int, default=20000)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--e2e-steps', type=int, default=2)
+    args = ap.parse_args()
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        return run_reference(args, rank)
+
+    # CPU baseline first: its spawn pool starts before any GPU work
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(n_steps=args.cpu_steps)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sw = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk).configure()
+    batch = sw.build()
+    batch.snapshot()
+    n_steps = sw.n_steps
+    launches_per_step = int(np.ceil(n_steps / (args.chunk or n_steps))) + 1
+    nnz = sw._sim._conn.nnz
+    st = torch.cuda.current_stream()
+
+    def one_step():
+        batch.reset()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(st)
+        sw.run_device()
+        e1.record(st)
+        fc = sw.fc_device()
+        e2.record(st)
+        return e0, e1, e2, fc
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    wall0 = time.perf_counter()
+    evs = [one_step() for _ in range(args.steps)]
+    barrier()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop()
+    step_ms = [e0.elapsed_time(e2) for e0, e1, e2, _ in evs]
+    kern_ms = [e0.elapsed_time(e1) for e0, e1, e2, _ in evs]
+    t_dev = float(np.sum(step_ms)) / 1e3
+    t_kern = float(np.mean(kern_ms)) / 1e3
+    status = batch.status()
+
+    # end to end through the public API: host inputs -> host Bold + FC
+    e2e_times, h2d, d2h = [], 0, 0
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(st)
+        sw2 = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk).configure()
+        res = sw2.run(fc=True)
+        s1.record(st)
+        torch.cuda.synchronize()
+        e2e_times.append(s0.elapsed_time(s1) / 1e3)
+        h2d, d2h = sw2.batch.h2d_bytes, sw2.batch.d2h_bytes + res['fc'].nbytes
+        del sw2, res
+
+    if world > 1:
+        tt = torch.tensor([t_dev, t_kern, float(np.median(e2e_times))], device='cuda', dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev, t_kern, t_e2e = tt.tolist()
+    else:
+        t_e2e = float(np.median(e2e_times))
+
+    region_steps = float(args.instances) * n_steps * N_REGIONS * world
+    value = region_steps * args.steps / t_dev
+    gather_bytes = float(args.instances) * n_steps * 4.0 * nnz
+    peaks = {}
+    try:
+        with open(os.path.join(HERE, 'MEASURED_PEAKS.json')) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = float(peaks.get('hbm_gbs', 6650.0))
+    achieved = gather_bytes / t_kern / 1e9
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * t_dev / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'rww_sweep_68r_1024i_60s_bold_fc', 'instances_per_gpu': args.instances,
+                       'regions': N_REGIONS, 'nnz': nnz, 'dt_ms': DT, 'sim_ms': args.length, 'steps': n_steps,
+                       'bold_tr_ms': 2000.0, 'fc': True, 'noise': 'philox',
+                       'parallelism': 'instances sharded over ranks' if world > 1 else 'single gpu',
+                       'l2': 'flushed between steps by the per-step state reset (%.1f GB written)'
+                             % ((batch.init.size + batch.zero.size + batch.out.size) / 1e9),
+                       'ring_in_smem': batch.ring_in_smem, 'sync_every': batch.sync_every},
+            'e2e': {'value': region_steps / t_e2e, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d),
+                    'd2h_bytes_per_step': int(d2h)},
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': None,
+                         'note': 'algorithmic gather bytes 4*ncvar*nnz per instance-step over the simulation '
+                                 'kernel time; peak = measured HBM copy bandwidth'},
+            'gpu_launches': launches_per_step * args.steps,
+            'kernel_ms_per_step': 1e3 * t_kern,
+            'nonfinite_instances': int((status != 0).sum()),
+            'wall_s_timed': wall,
+        }
+        if clocks:
+            line['clocks'] = clocks
+        if cb:
+            line['cpu_baseline'] = cb
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -144,7 +144,7 @@ class Batch:
     # ------------------------------------------------------------------ build
     def _build(self):
         specs, nvoi = self.specs, self.nvoi
-        init, zero = _Arena(), _Arena()
+        init, zero, outa = _Arena(), _Arena(), _Arena()
         conns = {}
         for s in specs:
             if id(s.conn) not in conns:
@@ -177,14 +177,14 @@ class Batch:
             s1 = s.step0 + s.n_steps
             if s.raw:
                 m['raw_rows'] = s.n_steps
-                zero.add(('raw', k), s.n_steps * nvoi * n * 4)
+                outa.add(('raw', k), s.n_steps * nvoi * n * 4)
             if s.tavg_istep:
                 m['tavg_rows'] = s1 // s.tavg_istep - s.step0 // s.tavg_istep
-                zero.add(('tavg', k), max(m['tavg_rows'], 1) * nvoi * n * 4)
+                outa.add(('tavg', k), max(m['tavg_rows'], 1) * nvoi * n * 4)
             if s.bold is not None:
                 bi = s.bold['istep']
                 m['bold_rows'] = s1 // bi - s.step0 // bi
-                zero.add(('bold', k), max(m['bold_rows'], 1) * nvoi * n * 8)
+                outa.add(('bold', k), max(m['bold_rows'], 1) * nvoi * n * 8)
             self.meta.append(m)
         init.add(('insts',), len(specs) * _lib.INST_DTYPE.itemsize)
         zero.add(('status',), len(specs) * 4)
@@ -192,8 +192,9 @@ class Batch:
         dev = self.device
         self.init_buf = torch.empty(max(init.size, 1), dtype=torch.uint8, device=dev)
         self.zero_buf = torch.zeros(max(zero.size, 1), dtype=torch.uint8, device=dev)
-        ib, zb = self.init_buf.data_ptr(), self.zero_buf.data_ptr()
-        self.init, self.zero = init, zero
+        self.out_buf = torch.zeros(max(outa.size, 1), dtype=torch.uint8, device=dev)
+        ib, zb, ob = self.init_buf.data_ptr(), self.zero_buf.data_ptr(), self.out_buf.data_ptr()
+        self.init, self.zero, self.out = init, zero, outa
 
         stage = np.zeros(max(init.size, 1), dtype=np.uint8)
 
@@ -204,6 +205,8 @@ class Batch:
             return ib + off
 
         def zaddr(key):
+            if key in outa.regions:
+                return ob + outa.regions[key][0]
             if key in zero.regions:
                 return zb + zero.regions[key][0]
             if key in init.regions:
@@ -274,6 +277,27 @@ class Batch:
         self.steps_done = 0
         self.max_total = max(s.n_steps for s in specs)
 
+    # ------------------------------------------------------------------ reset
+    def snapshot(self):
+        """Keep a device copy of the uploaded inputs so that reset() can restart
+        the batch from its initial state without a host transfer."""
+        self._pristine = self.init_buf.clone()
+
+    def reset(self):
+        """Restart every instance from its initial state (device-to-device)."""
+        self.init_buf.copy_(self._pristine)
+        self.zero_buf.zero_()
+        self.out_buf.zero_()
+        self.steps_done = 0
+
+    @property
+    def h2d_bytes(self):
+        return self.init.size + sum(int(f.numel()) * 4 for f in self._fed)
+
+    @property
+    def d2h_bytes(self):
+        return self.out.size
+
     # -------------------------------------------------------------------- run
     def launch_struct(self, max_steps):
         L = _lib.Launch()
@@ -311,6 +335,11 @@ class Batch:
         t = self.zero_buf[off:off + nb].view(dtype)
         return t[:int(np.prod(shape))].view(*shape)
 
+    def _oview(self, key, dtype, shape):
+        off, nb = self.out.regions[key]
+        t = self.out_buf[off:off + nb].view(dtype)
+        return t[:int(np.prod(shape))].view(*shape)
+
     def _iview(self, key, dtype, shape):
         off, nb = self.init.regions[key]
         t = self.init_buf[off:off + nb].view(dtype)
@@ -322,16 +351,16 @@ class Batch:
         m, nvoi = self.meta[k], self.nvoi
         out = {}
         if 'raw_rows' in m:
-            out['raw'] = self._zview(('raw', k), torch.float32, (m['raw_rows'], nvoi, m['n']))
+            out['raw'] = self._oview(('raw', k), torch.float32, (m['raw_rows'], nvoi, m['n']))
         if 'tavg_rows' in m:
-            out['tavg'] = self._zview(('tavg', k), torch.float32, (m['tavg_rows'], nvoi, m['n']))
+            out['tavg'] = self._oview(('tavg', k), torch.float32, (m['tavg_rows'], nvoi, m['n']))
         if 'bold_rows' in m:
-            out['bold'] = self._zview(('bold', k), torch.float64, (m['bold_rows'], nvoi, m['n']))
+            out['bold'] = self._oview(('bold', k), torch.float64, (m['bold_rows'], nvoi, m['n']))
         return out
 
     def outputs_host(self):
         """All outputs of all instances as numpy arrays, from one device-to-host copy."""
-        host = self.zero_buf.cpu().numpy()
+        host = self.out_buf.cpu().numpy()
         res = []
         for k, m in enumerate(self.meta):
             o = {}
@@ -339,7 +368,7 @@ class Batch:
             for key, dt, rows in (('raw', np.float32, 'raw_rows'), ('tavg', np.float32, 'tavg_rows'),
                                   ('bold', np.float64, 'bold_rows')):
                 if rows in m:
-                    off, nb = self.zero.regions[(key, k)]
+                    off, nb = self.out.regions[(key, k)]
                     cnt = m[rows] * nvoi * n
                     o[key] = host[off:off + nb].view(dt)[:cnt].reshape(m[rows], nvoi, n)
             res.append(o)

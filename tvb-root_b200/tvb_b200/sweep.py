@@ -1,0 +1,145 @@
+"""Batched parameter sweeps: many instances of one simulation configuration in
+one kernel launch, differing in coupling strength, noise and model
+parameters.
+
+Each instance is what the reference would run as a separate
+``Simulator(...).configure().run()`` (one process per grid point in the
+framework's parameter-space exploration); here they all advance together,
+one CTA each, sharing the connectome on the device.  Initial histories are
+drawn exactly as the reference draws them for each instance.  The Bold
+output of every instance can be reduced to its functional connectivity
+(Pearson over time, float64) on the device.
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import Batch, Connectome, InstanceSpec, functional_connectivity
+from .simulator import (Simulator, adopt_connectivity, adopt_coupling, adopt_integrator, adopt_model,
+                        adopt_monitor, noise_sigma)
+from . import monitors as monitors_mod
+
+
+class ParameterSweep:
+    """Sweep of `n_instances` simulations.
+
+    sweep: dict mapping 'coupling.<name>', 'noise.nsig' or 'model.<name>' to
+    arrays of one value per instance.  Noise: 'philox' draws an independent
+    device stream per instance (key = (noise_seed, instance index));
+    'reference' feeds every instance the reference's RandomState stream (the
+    same for all, as separate reference runs with the default seed would
+    draw), which is for parity checks on short runs.
+    """
+
+    def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
+                 noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None):
+        self.model = adopt_model(model)
+        self.connectivity = adopt_connectivity(connectivity)
+        self.coupling = adopt_coupling(coupling)
+        self.integrator = adopt_integrator(integrator)
+        self.monitors = [adopt_monitor(m) for m in (monitors if isinstance(monitors, (list, tuple)) else [monitors])]
+        self.simulation_length = float(simulation_length)
+        self.sweep = {k: np.atleast_1d(np.asarray(v, dtype=np.float64)) for k, v in sweep.items()}
+        sizes = {v.size for v in self.sweep.values()}
+        if len(sizes) != 1:
+            raise ValueError('all swept parameters need the same number of values')
+        self.n_instances = sizes.pop()
+        self.noise_source = noise_source
+        self.chunk_steps = chunk_steps
+        self.device = device
+        self.sync_every = sync_every
+        self.ring_in_smem = ring_in_smem
+        self.batch = None
+
+    def configure(self):
+        # one reference-equivalent simulator resolves delays, history and monitors
+        self._sim = Simulator(model=self.model, connectivity=self.connectivity, coupling=self.coupling,
+                              integrator=self.integrator, monitors=self.monitors,
+                              simulation_length=self.simulation_length, noise_source=self.noise_source,
+                              device=self.device).configure()
+        sim = self._sim
+        self.n_steps = int(np.ceil(self.simulation_length / self.integrator.dt))
+        n = sim.number_of_nodes
+        conn = sim._conn
+        raw, tavg_istep, bspec = sim._monitor_spec()
+        base_params = sim._params
+        pidx = {name: k for k, name in enumerate(self.model.kernel_param_names)}
+        cnames = list(type(self.coupling)._defaults)
+        fed = None
+        if self.integrator.stochastic and self.noise_source == 'reference':
+            z = self.integrator.noise.random_stream.normal(size=(self.n_steps, sim.nint, n)).astype(np.float32)
+            fed = torch.from_numpy(z)
+        self._fed = fed
+        specs = []
+        for i in range(self.n_instances):
+            params = base_params
+            cf = self.coupling.kernel_params()
+            sigma = sim._sigma
+            for key, vals in self.sweep.items():
+                part, name = key.split('.', 1)
+                if part == 'model':
+                    if params is base_params:
+                        params = base_params.copy()
+                    params[pidx[name]] = np.float32(vals[i])
+                elif part == 'coupling':
+                    cf = list(cf)
+                    cf[cnames.index(name)] = float(vals[i])
+                elif part == 'noise' and name == 'nsig':
+                    sigma = noise_sigma(np.array([vals[i]]), sim.nint, n, self.integrator.dt)
+                else:
+                    raise ValueError('cannot sweep %s' % key)
+            spec = InstanceSpec(conn, sim.history_buffer[..., 0], sim.current_state[..., 0], params, cf,
+                                self.n_steps, step0=sim.current_step, sigma=sigma, noise_fed=None,
+                                seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
+                                stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec)
+            specs.append(spec)
+        self._specs = specs
+        noise_kind = _lib.NOISE_NONE
+        if self.integrator.stochastic:
+            noise_kind = _lib.NOISE_FED if fed is not None else _lib.NOISE_PHILOX
+        self._noise_kind = noise_kind
+        return self
+
+    def build(self):
+        """Allocate the device batch and upload inputs (one host-to-device copy)."""
+        sim = self._sim
+        self.batch = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
+                           sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
+                           ring_in_smem=self.ring_in_smem)
+        if self._fed is not None:
+            fed = self._fed.to(self.batch.device).contiguous()
+            self.batch._fed.append(fed)
+            ins = self.batch.insts_host
+            ins['noise_fed'] = fed.data_ptr()
+            off, _ = self.batch.init.regions[('insts',)]
+            self.batch.init_buf[off:off + ins.nbytes].copy_(torch.from_numpy(ins.view(np.uint8)))
+        return self.batch
+
+    def run_device(self):
+        """Advance every instance to the end on the device (inputs already resident)."""
+        self.batch.run(chunk=self.chunk_steps)
+
+    def bold_device(self, voi=0):
+        """(I, T, n) float64 device tensor of the Bold series of one observed variable."""
+        return torch.stack([self.batch.outputs_device(i)['bold'][:, voi, :] for i in range(self.n_instances)])
+
+    def fc_device(self, voi=0):
+        """Per-instance functional connectivity (I, n, n) float64 on the device."""
+        bold = self.bold_device(voi)
+        return functional_connectivity(bold)
+
+    def run(self, fc=True):
+        """Build, run and return host results: dict with per-monitor arrays
+        (I, T, nvoi, n) under 'raw' / 'tavg' / 'bold' and 'fc' (I, n, n)."""
+        if self.batch is None:
+            self.build()
+        self.run_device()
+        res = {}
+        if fc and any(isinstance(m, monitors_mod.Bold) for m in self.monitors):
+            res['fc'] = self.fc_device().cpu().numpy()
+        outs = self.batch.outputs_host()
+        for key in ('raw', 'tavg', 'bold'):
+            if key in outs[0]:
+                res[key] = np.stack([o[key] for o in outs])
+        res['status'] = self.batch.status()
+        return res
