@@ -73,6 +73,13 @@ __global__ void gather_kernel(const tvbk_edge* __restrict__ edges, const float* 
 
 }  // namespace
 
+namespace tvbk {
+int set_error(int code, const char* msg) {
+    g_last_error = msg;
+    return code;
+}
+}  // namespace tvbk
+
 // --------------------------------------------------------------------- ABI
 
 extern "C" {

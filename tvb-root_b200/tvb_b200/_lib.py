@@ -26,6 +26,7 @@ SCHEME_IDS = {'EulerDeterministic': 0, 'EulerStochastic': 1, 'HeunDeterministic'
 NOISE_NONE, NOISE_FED, NOISE_PHILOX = 0, 1, 2
 MAX_REGIONS = 1024
 MAX_VOI = 8
+STATIC_SCRATCH_BYTES = 8 * 1024 * 1024
 
 
 class Edge(ctypes.Structure):
@@ -109,6 +110,7 @@ _SIGNATURES = {
     'tvbk_sim_run': (_I32, [ctypes.POINTER(Launch), _P]),
     'tvbk_gather_delayed': (_I32, [ctypes.POINTER(Inst), _I32, _I64, _P, _P]),
     'tvbk_fc': (_I32, [_P, _I32, _I32, _I32, _P, _P]),
+    'tvbk_sim_run_static': (_I32, [ctypes.POINTER(Launch), ctypes.POINTER(Inst), _P, _P]),
 }
 
 EXPORTED = tuple(_SIGNATURES)
