@@ -48,6 +48,7 @@ extern "C" {
 
 /* per-instance status bits written by the simulation kernel */
 #define TVBK_STATUS_NONFINITE 1   /* a state variable became NaN or Inf */
+#define TVBK_STATUS_DEGREE 2      /* a row had more edges than launch.max_degree (coupling incomplete) */
 
 /* components */
 enum {
@@ -137,6 +138,7 @@ typedef struct tvbk_launch {
     int32_t max_ring_len;        /* largest ring_len; the ring is staged in shared memory if it fits */
     int32_t sync_every;          /* barrier interval K, 1 <= K <= min(d_min + 1, ring_len - horizon) */
     int32_t ring_in_smem;        /* 1: stage rings in shared memory (needs fit), 0: read them in place */
+    int32_t max_degree;          /* largest row degree (non-zero weights of a target region) over the instances */
     int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */
     float dt;
 } tvbk_launch;

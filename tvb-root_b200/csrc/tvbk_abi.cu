@@ -193,6 +193,7 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (L->voi[v] < 0 || L->voi[v] >= d.nobs)
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: voi %d out of range", L->voi[v]);
     if (L->sync_every < 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: sync_every must be >= 1");
+    if (L->max_degree < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_degree < 0");
     if (L->max_steps < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_steps < 0");
     if (!(L->dt > 0.0f)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: dt must be > 0");
     const bool stoch = L->scheme == TVBK_SCHEME_EULER_STOCH || L->scheme == TVBK_SCHEME_HEUN_STOCH;

@@ -5,8 +5,8 @@ namespace tvbk {
 
 int launch_g2d(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
     switch (L.cfun) {
-        case CF_LINEAR: return launch_cfun<G2D, CF_LINEAR>(L, st, smem_bytes);
-        case CF_DIFFERENCE: return launch_cfun<G2D, CF_DIFFERENCE>(L, st, smem_bytes);
+        case CF_LINEAR: return launch_cfun<G2D, CF_LINEAR>(L, st, smem_bytes, L.max_degree);
+        case CF_DIFFERENCE: return launch_cfun<G2D, CF_DIFFERENCE>(L, st, smem_bytes, L.max_degree);
         default: return -2;
     }
 }

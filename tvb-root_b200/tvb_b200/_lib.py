@@ -18,6 +18,7 @@ TVBK_ERR_UNSUPPORTED = -2
 TVBK_ERR_CUDA = -3
 TVBK_ERR_TOO_LARGE = -4
 TVBK_STATUS_NONFINITE = 1
+TVBK_STATUS_DEGREE = 2
 
 MODEL_IDS = {'Generic2dOscillator': 0, 'JansenRit': 1, 'ReducedWongWang': 2, 'Epileptor': 3, 'Sum': 4}
 CFUN_IDS = {'Linear': 0, 'Difference': 1, 'SigmoidalJansenRit': 2}
@@ -85,6 +86,7 @@ class Launch(ctypes.Structure):
         ('max_ring_len', ctypes.c_int32),
         ('sync_every', ctypes.c_int32),
         ('ring_in_smem', ctypes.c_int32),
+        ('max_degree', ctypes.c_int32),
         ('max_steps', ctypes.c_int64),
         ('dt', ctypes.c_float),
     ]

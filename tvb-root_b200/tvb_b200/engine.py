@@ -125,6 +125,7 @@ class Batch:
         K = dmin + 1 if sync_every is None else int(sync_every)
         K = max(1, min(K, dmin + 1))
         self.max_n = max(s.conn.n for s in self.specs)
+        self.max_degree = max(int(np.diff(s.conn.row_ptr).max()) if s.conn.nnz else 0 for s in self.specs)
         if self.max_n > _lib.MAX_REGIONS:
             raise ValueError('%d regions exceed this build (%d)' % (self.max_n, _lib.MAX_REGIONS))
         hmax = max(s.conn.horizon for s in self.specs)
@@ -312,6 +313,7 @@ class Batch:
         L.max_ring_len = max(m['ring_len'] for m in self.meta)
         L.sync_every = self.sync_every
         L.ring_in_smem = 1 if self.ring_in_smem else 0
+        L.max_degree = self.max_degree
         L.max_steps = int(max_steps)
         L.dt = self.dt
         return L
