@@ -45,7 +45,7 @@ def sweep_grid():
     return gg.reshape(-1), ss.reshape(-1)
 
 
-def make_sweep(instances, length_ms, rank=0, chunk=None):
+def make_sweep(instances, length_ms, rank=0, chunk=None, gather='auto', lanes=1):
     from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
     from tvb_b200.connectivity import Connectivity
     from tvb_b200.sweep import ParameterSweep
@@ -56,7 +56,7 @@ def make_sweep(instances, length_ms, rank=0, chunk=None):
                         coupling=coupling.Linear(), monitors=[monitors.Bold(period=2000.0)],
                         integrator=integrators.EulerStochastic(dt=DT, noise=noise.Additive(nsig=[1e-3])),
                         simulation_length=length_ms, sweep={'coupling.a': G[idx], 'noise.nsig': S[idx]},
-                        chunk_steps=chunk)
+                        chunk_steps=chunk, gather=gather, lanes=lanes)
     return sw
 
 
@@ -181,6 +181,11 @@ def main():
     ap.add_argument('--cpu-steps', type=int, default=20000)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-steps', type=int, default=2)
+    ap.add_argument('--gather', default='auto', choices=['auto', 'row', 'edge'],
+                    help='coupling gather variant of the simulation kernel')
+    ap.add_argument('--lanes', default='1', choices=['auto', '1', '2', '4', '8'],
+                    help='instance groups (interleaved rings, one thread per region and instance) or one '
+                         'instance per CTA')
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -206,7 +211,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    sw = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk).configure()
+    sw = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk, gather=args.gather,
+                    lanes=args.lanes if args.lanes == 'auto' else int(args.lanes)).configure()
     batch = sw.build()
     batch.snapshot()
     n_steps = sw.n_steps
@@ -244,12 +250,13 @@ def main():
 
     # end to end through the public API: host inputs -> host Bold + FC
     e2e_times, h2d, d2h = [], 0, 0
-    for _ in range(args.e2e_steps):
+    for _ in range(max(args.e2e_steps, 0)):
         torch.cuda.synchronize()
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
         s0.record(st)
-        sw2 = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk).configure()
+        sw2 = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk, gather=args.gather,
+                    lanes=args.lanes if args.lanes == 'auto' else int(args.lanes)).configure()
         res = sw2.run(fc=True)
         s1.record(st)
         torch.cuda.synchronize()
@@ -257,6 +264,8 @@ def main():
         h2d, d2h = sw2.batch.h2d_bytes, sw2.batch.d2h_bytes + res['fc'].nbytes
         del sw2, res
 
+    if not e2e_times:
+        e2e_times = [float('inf')]
     if world > 1:
         tt = torch.tensor([t_dev, t_kern, float(np.median(e2e_times))], device='cuda', dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -286,7 +295,10 @@ def main():
                        'parallelism': 'instances sharded over ranks' if world > 1 else 'single gpu',
                        'l2': 'flushed between steps by the per-step state reset (%.1f GB written)'
                              % ((batch.init.size + batch.zero.size + batch.out.size) / 1e9),
-                       'ring_in_smem': batch.ring_in_smem, 'sync_every': batch.sync_every},
+                       'ring_in_smem': batch.ring_in_smem, 'sync_every': batch.sync_every,
+                       'gather': 'edge-parallel %d/thread, %d threads' % (batch.edges_per_thread, batch.block_threads)
+                                 if batch.edges_per_thread else 'row per thread',
+                       'lanes': batch.lanes, 'prefetch': batch.prefetch},
             'e2e': {'value': region_steps / t_e2e, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d),
                     'd2h_bytes_per_step': int(d2h)},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',

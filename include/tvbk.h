@@ -139,6 +139,21 @@ typedef struct tvbk_launch {
     int32_t sync_every;          /* barrier interval K, 1 <= K <= min(d_min + 1, ring_len - horizon) */
     int32_t ring_in_smem;        /* 1: stage rings in shared memory (needs fit), 0: read them in place */
     int32_t max_degree;          /* largest row degree (non-zero weights of a target region) over the instances */
+    int32_t edges_per_thread;    /* 0: one thread per row; 8, 12, 16 or 24: edge-parallel gather with that many
+                                  * register slots per thread (rings in shared memory, Linear or
+                                  * SigmoidalJansenRit only; ceil(nnz / block_threads) must not exceed it nor
+                                  * the smallest non-zero row degree of any instance) */
+    int32_t block_threads;       /* CTA size for the edge-parallel gather (multiple of 32, >= max_n, <= 512) */
+    int32_t prefetch;            /* 1: issue the gather of step s + 1 before the update of step s (row kernel,
+                                  * Linear or SigmoidalJansenRit); needs every delay >= 1 and
+                                  * 1 <= sync_every <= the smallest delay */
+    int32_t lanes;               /* 1, or 8 / ncvar: instance groups.  Consecutive groups of `lanes` instances
+                                  * share connectome, ring length and step range; one thread advances one
+                                  * (region, instance) pair and the group's rings are interleaved
+                                  * [ring_len][n][ncvar][lanes] in the `ring` of the group's first instance,
+                                  * read in place (regions * lanes <= 1024 threads; the edge list and two
+                                  * staging buffers of max_degree * ncvar floats per thread must fit in
+                                  * shared memory) */
     int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */
     float dt;
 } tvbk_launch;

@@ -264,3 +264,61 @@ def test_philox_stream_matches_oracle():
                         {'a': fx['G'][3]}, 'EulerStochastic', n_steps, [O.Monitor('TemporalAverage', 100.0)],
                         buf0, st0, 0, nsig=[fx['nsig'][3]], noise_z=z)
     report('philox rww tavg vs oracle', tavg[..., 0], out[0][1], 1e-4)
+
+
+@pytest.mark.parametrize('cfun', ['Linear', 'SigmoidalJansenRit', 'Difference'])
+def test_kernel_variants_agree(cfun):
+    """The row kernel, the edge-parallel kernel (balanced edge split, row
+    partials) and the instance-lane kernels (2 and 4 interleaved instances,
+    rings in shared or global memory) compute the same trajectories up to
+    float32 summation order."""
+    import bench
+    from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.sweep import ParameterSweep
+    if cfun == 'Linear':
+        w, L = synthetic.connectome(68, 0.3, 10.0, 200.0, seed=3)
+        model, cf = models.ReducedWongWang(), coupling.Linear()
+
+        def integ():  # a fresh RandomState per run: it draws the initial history
+            return integrators.EulerStochastic(dt=0.1, noise=noise.Additive(nsig=[1e-3]))
+        sweep = {'coupling.a': np.logspace(-2, 0, 8), 'noise.nsig': np.logspace(-4, -3, 8)}
+        mons, length = [monitors.TemporalAverage(period=10.0), monitors.Bold(period=2000.0)], 4000.0
+    elif cfun == 'Difference':
+        w, L = synthetic.connectome(40, 0.4, 5.0, 60.0, seed=9)
+        model, cf = models.Epileptor(Ks=np.array([-0.2]), Kf=np.array([0.05])), coupling.Difference()
+
+        def integ():
+            return integrators.HeunDeterministic(dt=0.05)
+        sweep = {'coupling.a': np.linspace(0.05, 0.2, 8)}
+        mons, length = [monitors.TemporalAverage(period=1.0)], 20.0
+    else:
+        w, L = synthetic.connectome(48, 0.4, 5.0, 60.0, seed=8)
+        model, cf = models.JansenRit(), coupling.SigmoidalJansenRit()
+
+        def integ():
+            return integrators.HeunDeterministic(dt=0.05)
+        sweep = {'coupling.a': np.linspace(0.5, 2.0, 8)}
+        mons, length = [monitors.TemporalAverage(period=1.0)], 200.0
+    out = {}
+    variants = [('row', 1, None), ('row', 1, False), ('row', 'auto', None)]
+    if cfun != 'Difference':
+        variants.append(('edge', 1, None))
+    for gather, lanes, smem in variants:
+        np.random.seed(11)
+        sw = ParameterSweep(model=model, connectivity=Connectivity(w, L, speed=5.0), coupling=cf, integrator=integ(),
+                            monitors=mons, simulation_length=length, sweep=sweep, gather=gather, lanes=lanes,
+                            ring_in_smem=smem).configure()
+        res = sw.run(fc=False)
+        assert (res['status'] == 0).all()
+        key = (gather, sw.batch.lanes, sw.batch.ring_in_smem)
+        if lanes == 'auto':
+            assert sw.batch.lanes == 8 // sw.batch.ncvar
+        if gather == 'edge':
+            assert sw.batch.edges_per_thread > 0
+        out[key] = res
+    base = out[('row', 1, True)]
+    for key, res in out.items():
+        for mon in ('tavg', 'bold'):
+            if mon in res and key != ('row', 1, True):
+                report('%s %s %s vs row' % (cfun, mon, key), res[mon], base[mon], 1e-5)

@@ -194,6 +194,7 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: voi %d out of range", L->voi[v]);
     if (L->sync_every < 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: sync_every must be >= 1");
     if (L->max_degree < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_degree < 0");
+    if (L->prefetch != 0 && L->prefetch != 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch must be 0 or 1");
     if (L->max_steps < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_steps < 0");
     if (!(L->dt > 0.0f)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: dt must be > 0");
     const bool stoch = L->scheme == TVBK_SCHEME_EULER_STOCH || L->scheme == TVBK_SCHEME_HEUN_STOCH;
@@ -201,7 +202,42 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: stochastic scheme needs fed or Philox noise");
     if (L->max_steps == 0) return TVBK_OK;
     size_t smem = 0;
-    if (L->ring_in_smem) {
+    if (L->lanes > 1) {
+        if (L->lanes * d.ncvar != 8)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: instance groups have 8 / ncvar = %d lanes", 8 / d.ncvar);
+        if (L->n_inst % L->lanes != 0)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: %d instances are not groups of %d", L->n_inst, L->lanes);
+        if (L->edges_per_thread != 0 || L->ring_in_smem)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: instance groups read their rings in place and use the "
+                        "row gather");
+        if (L->model == TVBK_MODEL_SUM) return fail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run: groups with the Sum model");
+        const int64_t threads = ((int64_t)L->max_n * L->lanes + 31) / 32 * 32;
+        const int64_t b = ((int64_t)L->max_n * L->max_degree * 8 + 15) / 16 * 16 +
+                          (int64_t)2 * L->max_degree * d.ncvar * threads * 4;
+        if (threads > 1024 || b > kMaxSmemPerBlock)
+            return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: a group of %d lanes x %d regions needs %lld threads and "
+                        "%lld bytes of shared memory", L->lanes, L->max_n, (long long)threads, (long long)b);
+    } else if (L->edges_per_thread != 0) {
+        const int E = L->edges_per_thread;
+        if (E != 8 && E != 12 && E != 16 && E != 24)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: edges_per_thread must be 0, 8, 12, 16 or 24");
+        if (L->cfun == TVBK_CFUN_DIFFERENCE)
+            return fail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run: the edge-parallel gather needs Linear or "
+                        "SigmoidalJansenRit coupling");
+        if (!L->ring_in_smem) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: the edge-parallel gather needs rings "
+                                          "in shared memory");
+        if (L->block_threads < L->max_n || L->block_threads > 512 || L->block_threads % 32 != 0)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: block_threads %d must be a multiple of 32 in [max_n, 512]",
+                        L->block_threads);
+        if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
+        const int64_t ring = ((int64_t)L->max_ring_len * L->max_n * d.ncvar + 3) / 4 * 4;
+        const int nacc = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
+        const int64_t b = (ring + (int64_t)2 * L->block_threads * 2 * nacc) * (int64_t)sizeof(float);
+        if (b > kMaxSmemPerBlock)
+            return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: ring and partials need %lld bytes of shared memory",
+                        (long long)b);
+        smem = (size_t)b;
+    } else if (L->ring_in_smem) {
         if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
         const int64_t b = (int64_t)L->max_ring_len * L->max_n * d.ncvar * (int64_t)sizeof(float);
         if (b > kMaxSmemPerBlock || L->max_n > 256)

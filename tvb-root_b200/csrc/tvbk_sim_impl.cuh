@@ -35,6 +35,10 @@ struct SchemeTraits {
     static constexpr bool stoch = (SCHEME == TVBK_SCHEME_EULER_STOCH || SCHEME == TVBK_SCHEME_HEUN_STOCH);
 };
 
+// True at the first step of a launch and at every step s with s & 3 == 0:
+// where a new block of four Philox normals starts.
+#define STOCH_BLOCK_START(ks) ((ks) == 0 || ((s0 + 1 + (ks)) & 3) == 0)
+
 // acc += w * pre(x_i, x_j) for one edge whose delayed value(s) start at src.
 template <int CF, int NCV>
 __device__ __forceinline__ void accumulate(float* acc, float w, const float* src, const float* xi, const float* cf) {
@@ -93,7 +97,7 @@ struct RegRow {
 #pragma unroll
         for (int k = 0; k < MAXD; ++k) {
             const int2 ed = (k < deg) ? __ldg(ed2 + k) : make_int2(0, 0);
-            off[k] = ed.x;
+            off[k] = ed.x * (int)sizeof(float);  // byte offsets: no scaling per edge
             w[k] = __int_as_float(ed.y);
         }
     }
@@ -104,10 +108,12 @@ struct RegRow {
         float a0[NCV], a1[NCV];
 #pragma unroll
         for (int k = 0; k < NCV; ++k) a0[k] = a1[k] = 0.0f;
+        const char* rb = reinterpret_cast<const char*>(ring);
+        const int base_b = base_off * (int)sizeof(float), ring_b = ring_floats * (int)sizeof(float);
 #pragma unroll
         for (int k = 0; k < MAXD; ++k) {
-            const int a = gather_addr(base_off, off[k], ring_floats);
-            accumulate<CF, NCV>((k & 1) ? a1 : a0, w[k], ring + a, xi, cf);
+            const int a = gather_addr(base_b, off[k], ring_b);
+            accumulate<CF, NCV>((k & 1) ? a1 : a0, w[k], reinterpret_cast<const float*>(rb + a), xi, cf);
         }
 #pragma unroll
         for (int k = 0; k < NCV; ++k) a0[k] += a1[k];
@@ -148,11 +154,228 @@ struct RegRow<M, CF, 0> {
     }
 };
 
-template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD>
+// Per-region state and update: scheme step with noise, ring write and the
+// monitors (shared by both kernel variants).
+template <class M, int SCHEME>
+struct Node {
+    static constexpr int NSV = M::NSV, NCV = M::NCV, NP = M::NP, NINT = M::NINT;
+    static constexpr bool STOCH = SchemeTraits<SCHEME>::stoch;
+    static constexpr int MV = M::NOBS < TVBK_MAX_VOI ? M::NOBS : TVBK_MAX_VOI;  // nvoi <= nobs checked on the host
+
+    float x[NSV], p[NP], sig[NINT], zc[NINT][4], tacc[MV];
+    double bacc[MV];
+    float* raw_p;
+    const float* fed_p;
+    float* tavg_p;
+    double* bold_p;
+    int ph_t, ph_b, ph_i, q_prev;
+    // descriptor fields used every step, held in registers: read through the
+    // descriptor pointer they would be reloaded after every store
+    int t_istep, b_istep, b_ii, SL;
+    double* stock;
+    const double* hrf;
+    double k1v0;
+    uint32_t seed, stream;
+
+    __device__ __forceinline__ void init(const tvbk_launch& L, const tvbk_inst* Ip, int i, int n, int64_t s0) {
+        const int nvoi = L.nvoi;
+#pragma unroll
+        for (int k = 0; k < NSV; ++k) x[k] = Ip->state[k * n + i];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) p[k] = Ip->params[k * n + i];
+#pragma unroll
+        for (int k = 0; k < NINT; ++k) sig[k] = STOCH ? Ip->noise_sigma[k * n + i] : 0.0f;
+#pragma unroll
+        for (int k = 0; k < NINT; ++k)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) zc[k][r] = 0.0f;
+        const bool do_tavg = Ip->tavg != nullptr, do_bold = Ip->bold != nullptr;
+#pragma unroll
+        for (int v = 0; v < MV; ++v) {
+            tacc[v] = (do_tavg && v < nvoi) ? Ip->tavg_acc[v * n + i] : 0.0f;
+            bacc[v] = (do_bold && v < nvoi) ? Ip->bold_acc[v * n + i] : 0.0;
+        }
+        t_istep = Ip->tavg_istep;
+        b_istep = Ip->bold_istep;
+        b_ii = Ip->bold_ii;
+        SL = Ip->stock_len;
+        stock = Ip->bold_stock;
+        hrf = Ip->hrf;
+        k1v0 = Ip->bold_k1v0;
+        seed = Ip->seed;
+        stream = Ip->stream;
+        // monitor phases (64-bit divisions once per launch)
+        ph_t = do_tavg ? (int)(s0 % Ip->tavg_istep) : 0;
+        ph_b = do_bold ? (int)(s0 % Ip->bold_istep) : 0;
+        ph_i = do_bold ? (int)(s0 % Ip->bold_ii) : 0;
+        q_prev = do_bold ? (int)((s0 / Ip->bold_ii) % Ip->stock_len) : 0;
+        raw_p = Ip->raw ? Ip->raw + (size_t)(s0 - Ip->raw_base) * nvoi * n + i : nullptr;
+        fed_p = Ip->noise_fed ? Ip->noise_fed + (size_t)(s0 - Ip->fed_base) * NINT * n + i : nullptr;
+        tavg_p = do_tavg ? Ip->tavg + (size_t)(s0 / Ip->tavg_istep - Ip->tavg_base) * nvoi * n + i : nullptr;
+        bold_p = do_bold ? Ip->bold + (size_t)(s0 / Ip->bold_istep - Ip->bold_base) * nvoi * n + i : nullptr;
+    }
+
+    // Philox normals of the 4-step block of step s (steps 4q .. 4q+3, q = s >> 2).
+    __device__ __forceinline__ void noise_block(const tvbk_launch& L, int i, int64_t s) {
+        if constexpr (STOCH) {
+            if (L.noise == TVBK_NOISE_PHILOX) {
+#pragma unroll
+                for (int k = 0; k < NINT; ++k)
+                    if (sig[k] != 0.0f) philox_normals4(seed, stream, s, i, k, zc[k]);
+            }
+        }
+    }
+
+    // One step s = s0 + 1 + ks with coupling input c.  The caller writes the
+    // new coupling variables x[cvar(k)] to the ring.
+    __device__ __forceinline__ void advance(const tvbk_launch& L, const tvbk_inst* Ip, int i, int n, int64_t s0,
+                                            int ks, const float* c) {
+        const float dt = L.dt;
+        const int nvoi = L.nvoi;
+        float z[NINT];
+        if constexpr (STOCH) {
+            if (L.noise == TVBK_NOISE_FED) {
+#pragma unroll
+                for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
+                fed_p += (size_t)NINT * n;
+            } else {
+                const int r = (int)((s0 + 1 + ks) & 3);
+#pragma unroll
+                for (int k = 0; k < NINT; ++k)
+                    z[k] = (r == 0) ? zc[k][0] : (r == 1) ? zc[k][1] : (r == 2) ? zc[k][2] : zc[k][3];
+            }
+        }
+
+        float m0[NSV];
+        M::dfun(x, c, p, m0);
+        if constexpr (SCHEME == TVBK_SCHEME_EULER_DET) {
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k];
+        } else if constexpr (SCHEME == TVBK_SCHEME_EULER_STOCH) {
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k] + sig[k] * z[k];
+        } else if constexpr (SCHEME == TVBK_SCHEME_HEUN_DET || SCHEME == TVBK_SCHEME_HEUN_STOCH) {
+            float inter[NSV], nz[NSV];
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) {
+                nz[k] = STOCH ? sig[k] * z[k] : 0.0f;
+                inter[k] = x[k] + dt * m0[k] + nz[k];
+            }
+            M::bound(inter);
+            float m1[NSV];
+            M::dfun(inter, c, p, m1);
+            const float hdt = dt * 0.5f;
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + (m0[k] + m1[k]) * hdt + nz[k];
+        } else {  // identity
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) x[k] = m0[k];
+        }
+        M::bound(x);
+
+        // monitors
+        if (raw_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) raw_p[v * n] = M::observe(L.voi[v], x);
+            raw_p += (size_t)nvoi * n;
+        }
+        if (tavg_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) tacc[v] += M::observe(L.voi[v], x);
+            if (++ph_t == t_istep) {
+                ph_t = 0;
+                const float inv_n = (float)t_istep;
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) {
+                        tavg_p[v * n] = tacc[v] / inv_n;
+                        tacc[v] = 0.0f;
+                    }
+                tavg_p += (size_t)nvoi * n;
+            }
+        }
+        if (bold_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) bacc[v] += (double)M::observe(L.voi[v], x);
+            if (++ph_i == b_ii) {
+                ph_i = 0;
+                double* st = stock + (size_t)q_prev * nvoi * n + i;
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) {
+                        st[v * n] = bacc[v] / (double)b_ii;
+                        bacc[v] = 0.0;
+                    }
+                q_prev = (q_prev + 1 == SL) ? 0 : q_prev + 1;
+            }
+            if (++ph_b == b_istep) {
+                ph_b = 0;
+                const int64_t s = s0 + 1 + ks;
+                const int m = (int)((s / b_ii) % SL);
+                // numpy.roll(hrf, m - 1)[k] == hrf[(k - m + 1) mod SL]
+                int idx0 = 1 - m;
+                idx0 = idx0 < 0 ? idx0 + SL : (idx0 >= SL ? idx0 - SL : idx0);
+                for (int v = 0; v < nvoi; ++v) {
+                    double dot = 0.0;
+                    int idx = idx0;
+                    const double* sv = stock + (size_t)v * n + i;
+                    for (int k = 0; k < SL; ++k) {
+                        dot = fma(__ldg(hrf + idx), sv[(size_t)k * nvoi * n], dot);
+                        idx = (idx + 1 == SL) ? 0 : idx + 1;
+                    }
+                    bold_p[v * n] = (dot - 1.0) * k1v0;
+                }
+                bold_p += (size_t)nvoi * n;
+            }
+        }
+    }
+
+    // history update: the coupling variables of the new state go to dst
+    __device__ __forceinline__ void write_ring(float* dst) const {
+        if constexpr (NCV == 1) {
+            dst[0] = x[M::cvar(0)];
+        } else {
+            *reinterpret_cast<float2*>(dst) = make_float2(x[M::cvar(0)], x[M::cvar(1)]);
+        }
+    }
+
+    __device__ __forceinline__ void finish(const tvbk_launch& L, tvbk_inst* Ip, int i, int n, int32_t* status) {
+        const int nvoi = L.nvoi;
+        bool finite = true;
+#pragma unroll
+        for (int k = 0; k < NSV; ++k) {
+            Ip->state[k * n + i] = x[k];
+            finite = finite && isfinite(x[k]);
+        }
+#pragma unroll
+        for (int v = 0; v < MV; ++v)
+            if (v < nvoi) {
+                if (Ip->tavg != nullptr) Ip->tavg_acc[v * n + i] = tacc[v];
+                if (Ip->bold != nullptr) Ip->bold_acc[v * n + i] = bacc[v];
+            }
+        if (!finite) atomicOr(status, TVBK_STATUS_NONFINITE);
+    }
+};
+
+__device__ __forceinline__ void stage_ring(float* dst, const float* src, int nfloats) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    const int n4 = nfloats >> 2;
+    for (int k = threadIdx.x; k < n4; k += blockDim.x) d4[k] = s4[k];
+    for (int k = (n4 << 2) + threadIdx.x; k < nfloats; k += blockDim.x) dst[k] = src[k];
+}
+
+// Row kernel: thread i gathers row i and advances region i.  With PIPE the
+// gather of step s + 1 is issued before the update of step s (it reads times
+// <= s - d_min only, so it does not wait for this step), which gives each
+// warp two independent instruction streams; it needs every delay >= 1, a
+// barrier interval K <= d_min, and a coupling whose pre() ignores x_i.
+template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE>
 __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
-    constexpr int NSV = M::NSV, NCV = M::NCV, NP = M::NP, NINT = M::NINT;
-    constexpr bool STOCH = SchemeTraits<SCHEME>::stoch;
-    constexpr int MV = M::NOBS < TVBK_MAX_VOI ? M::NOBS : TVBK_MAX_VOI;  // nvoi <= nobs is checked on the host
+    constexpr int NCV = M::NCV;
     extern __shared__ __align__(16) float smem[];
 
     tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x;
@@ -169,237 +392,204 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
 
     float* ring = SMEM ? smem : Ip->ring;
     if (SMEM) {
-        const float4* src = reinterpret_cast<const float4*>(Ip->ring);
-        float4* dst = reinterpret_cast<float4*>(smem);
-        const int n4 = ring_floats >> 2;
-        for (int k = i; k < n4; k += blockDim.x) dst[k] = src[k];
-        for (int k = (n4 << 2) + i; k < ring_floats; k += blockDim.x) smem[k] = Ip->ring[k];
+        stage_ring(smem, Ip->ring, ring_floats);
         __syncthreads();
     }
-
-    const float dt = L.dt;
-    const int nvoi = L.nvoi;
-    float x[NSV], p[NP], cf[6];
+    float cf[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) cf[k] = Ip->cfun[k];
     RegRow<M, CF, MAXD> row;
     row.deg = 0;
-    float sig[NINT];
-    float tacc[MV];
-    double bacc[MV];
-    float* raw = Ip->raw;
-    float* tavg = Ip->tavg;
-    double* bold = Ip->bold;
-    const bool do_tavg = tavg != nullptr, do_bold = bold != nullptr;
-#pragma unroll
-    for (int v = 0; v < MV; ++v) {
-        tacc[v] = 0.0f;
-        bacc[v] = 0.0;
-    }
+    Node<M, SCHEME> node;
     if (act) {
-#pragma unroll
-        for (int k = 0; k < NSV; ++k) x[k] = Ip->state[k * n + i];
-#pragma unroll
-        for (int k = 0; k < NP; ++k) p[k] = Ip->params[k * n + i];
         const int e0 = Ip->row_ptr[i], e1 = Ip->row_ptr[i + 1];
         if (MAXD > 0 && e1 - e0 > MAXD) atomicOr(L.status + blockIdx.x, TVBK_STATUS_DEGREE);
         row.load(Ip->edges, e0, e1);
-#pragma unroll
-        for (int k = 0; k < NINT; ++k) sig[k] = STOCH ? Ip->noise_sigma[k * n + i] : 0.0f;
-#pragma unroll
-        for (int v = 0; v < MV; ++v) {
-            if (v < nvoi) {
-                if (do_tavg) tacc[v] = Ip->tavg_acc[v * n + i];
-                if (do_bold) bacc[v] = Ip->bold_acc[v * n + i];
-            }
-        }
+        node.init(L, Ip, i, n, s0);
     }
-    // monitor phases (64-bit divisions once per launch)
-    const int t_istep = Ip->tavg_istep, b_istep = Ip->bold_istep, b_ii = Ip->bold_ii, SL = Ip->stock_len;
-    int ph_t = do_tavg ? (int)(s0 % t_istep) : 0;
-    int ph_b = do_bold ? (int)(s0 % b_istep) : 0;
-    int ph_i = do_bold ? (int)(s0 % b_ii) : 0;
-    int q_prev = do_bold ? (int)((s0 / b_ii) % SL) : 0;
-    float* raw_p = raw ? raw + (size_t)(s0 - Ip->raw_base) * nvoi * n + i : nullptr;
-    const float* fed_p = Ip->noise_fed ? Ip->noise_fed + (size_t)(s0 - Ip->fed_base) * NINT * n + i : nullptr;
-    float* tavg_p = do_tavg ? tavg + (size_t)(s0 / t_istep - Ip->tavg_base) * nvoi * n + i : nullptr;
-    double* bold_p = do_bold ? bold + (size_t)(s0 / b_istep - Ip->bold_base) * nvoi * n + i : nullptr;
-    const int noise_kind = L.noise;
-    const uint32_t seed = Ip->seed, stream = Ip->stream;
-    float zc[NINT][4];
-#pragma unroll
-    for (int k = 0; k < NINT; ++k)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) zc[k][r] = 0.0f;
-    int rphase = (int)((s0 + 1) & 3);  // s & 3 of the first step
-
     const int K = L.sync_every;
     int since_sync = 0;
     int wslot = (int)(s0 % RL);  // slot of the last written time
+    float cnext[NCV];
+    if (PIPE && act) row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
     for (int ks = 0; ks < nsteps; ++ks) {
-        const int base_off = wslot * slot_floats;  // time s - 1
+        const int prev = wslot;                     // slot of time s - 1
         wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
         if (act) {
-            float xi[NCV];
-#pragma unroll
-            for (int k = 0; k < NCV; ++k) xi[k] = x[M::cvar(k)];
+            if (STOCH_BLOCK_START(ks)) node.noise_block(L, i, s0 + 1 + ks);
             float c[NCV];
-            row.couple(ring, base_off, ring_floats, xi, cf, c);
-
-            float z[NINT];
-            if constexpr (STOCH) {
-                if (noise_kind == TVBK_NOISE_FED) {
+            if constexpr (PIPE) {
 #pragma unroll
-                    for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
-                    fed_p += (size_t)NINT * n;
-                } else {
-                    if (rphase == 0 || ks == 0) {
-                        const int64_t s = s0 + 1 + ks;
-#pragma unroll
-                        for (int k = 0; k < NINT; ++k)
-                            if (sig[k] != 0.0f) philox_normals4(seed, stream, s, i, k, zc[k]);
-                    }
-#pragma unroll
-                    for (int k = 0; k < NINT; ++k)
-                        z[k] = (rphase == 0) ? zc[k][0] : (rphase == 1) ? zc[k][1] : (rphase == 2) ? zc[k][2] : zc[k][3];
-                }
-            }
-
-            float m0[NSV];
-            M::dfun(x, c, p, m0);
-            if constexpr (SCHEME == TVBK_SCHEME_EULER_DET) {
-#pragma unroll
-                for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k];
-            } else if constexpr (SCHEME == TVBK_SCHEME_EULER_STOCH) {
-#pragma unroll
-                for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k] + sig[k] * z[k];
-            } else if constexpr (SCHEME == TVBK_SCHEME_HEUN_DET || SCHEME == TVBK_SCHEME_HEUN_STOCH) {
-                float inter[NSV], nz[NSV];
-#pragma unroll
-                for (int k = 0; k < NSV; ++k) {
-                    nz[k] = STOCH ? sig[k] * z[k] : 0.0f;
-                    inter[k] = x[k] + dt * m0[k] + nz[k];
-                }
-                M::bound(inter);
-                float m1[NSV];
-                M::dfun(inter, c, p, m1);
-                const float hdt = dt * 0.5f;
-#pragma unroll
-                for (int k = 0; k < NSV; ++k) x[k] = x[k] + (m0[k] + m1[k]) * hdt + nz[k];
-            } else {  // identity
-#pragma unroll
-                for (int k = 0; k < NSV; ++k) x[k] = m0[k];
-            }
-            M::bound(x);
-
-            // history update: coupling variables of time s
-            float* dst = ring + wslot * slot_floats + i * NCV;
-            if constexpr (NCV == 1) {
-                dst[0] = x[M::cvar(0)];
+                for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
+                // coupling of step s + 1: times s - d with d >= d_min >= 1
+                row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
             } else {
-                *reinterpret_cast<float2*>(dst) = make_float2(x[M::cvar(0)], x[M::cvar(1)]);
+                float xi[NCV];
+#pragma unroll
+                for (int k = 0; k < NCV; ++k) xi[k] = node.x[M::cvar(k)];
+                row.couple(ring, prev * slot_floats, ring_floats, xi, cf, c);
             }
-
-            // monitors
-            if (raw_p != nullptr) {
-#pragma unroll
-                for (int v = 0; v < MV; ++v)
-                    if (v < nvoi) raw_p[v * n] = M::observe(L.voi[v], x);
-                raw_p += (size_t)nvoi * n;
-            }
-            if (do_tavg) {
-#pragma unroll
-                for (int v = 0; v < MV; ++v)
-                    if (v < nvoi) tacc[v] += M::observe(L.voi[v], x);
-                if (++ph_t == t_istep) {
-                    ph_t = 0;
-#pragma unroll
-                    for (int v = 0; v < MV; ++v)
-                        if (v < nvoi) {
-                            tavg_p[v * n] = tacc[v] / (float)t_istep;
-                            tacc[v] = 0.0f;
-                        }
-                    tavg_p += (size_t)nvoi * n;
-                }
-            }
-            if (do_bold) {
-#pragma unroll
-                for (int v = 0; v < MV; ++v)
-                    if (v < nvoi) bacc[v] += (double)M::observe(L.voi[v], x);
-                double* stock = Ip->bold_stock;
-                if (++ph_i == b_ii) {
-                    ph_i = 0;
-                    double* st = stock + (size_t)q_prev * nvoi * n + i;
-#pragma unroll
-                    for (int v = 0; v < MV; ++v)
-                        if (v < nvoi) {
-                            st[v * n] = bacc[v] / (double)b_ii;
-                            bacc[v] = 0.0;
-                        }
-                    q_prev = (q_prev + 1 == SL) ? 0 : q_prev + 1;
-                }
-                if (++ph_b == b_istep) {
-                    ph_b = 0;
-                    const int64_t s = s0 + 1 + ks;
-                    const int m = (int)((s / b_ii) % SL);
-                    // numpy.roll(hrf, m - 1)[k] == hrf[(k - m + 1) mod SL]
-                    int idx0 = 1 - m;
-                    idx0 = idx0 < 0 ? idx0 + SL : (idx0 >= SL ? idx0 - SL : idx0);
-                    const double* __restrict__ hrf = Ip->hrf;
-                    const double k1v0 = Ip->bold_k1v0;
-                    for (int v = 0; v < nvoi; ++v) {
-                        double dot = 0.0;
-                        int idx = idx0;
-                        const double* sv = stock + (size_t)v * n + i;
-                        for (int k = 0; k < SL; ++k) {
-                            dot = fma(__ldg(hrf + idx), sv[(size_t)k * nvoi * n], dot);
-                            idx = (idx + 1 == SL) ? 0 : idx + 1;
-                        }
-                        bold_p[v * n] = (dot - 1.0) * k1v0;
-                    }
-                    bold_p += (size_t)nvoi * n;
-                }
-            }
+            node.advance(L, Ip, i, n, s0, ks, c);
+            node.write_ring(ring + wslot * slot_floats + i * NCV);
         }
-        rphase = (rphase + 1) & 3;
         if (++since_sync == K) {
             since_sync = 0;
             __syncthreads();
         }
     }
-
-    // write back
     __syncthreads();
-    if (act) {
-        bool finite = true;
-#pragma unroll
-        for (int k = 0; k < NSV; ++k) {
-            Ip->state[k * n + i] = x[k];
-            finite = finite && isfinite(x[k]);
-        }
-#pragma unroll
-        for (int v = 0; v < MV; ++v)
-            if (v < nvoi) {
-                if (do_tavg) Ip->tavg_acc[v * n + i] = tacc[v];
-                if (do_bold) Ip->bold_acc[v * n + i] = bacc[v];
-            }
-        if (!finite) atomicOr(L.status + blockIdx.x, TVBK_STATUS_NONFINITE);
-    }
-    if (SMEM) {
-        float4* dst = reinterpret_cast<float4*>(Ip->ring);
-        const float4* src = reinterpret_cast<const float4*>(smem);
-        const int n4 = ring_floats >> 2;
-        for (int k = i; k < n4; k += blockDim.x) dst[k] = src[k];
-        for (int k = (n4 << 2) + i; k < ring_floats; k += blockDim.x) Ip->ring[k] = smem[k];
-    }
+    if (act) node.finish(L, Ip, i, n, L.status + blockIdx.x);
+    if (SMEM) stage_ring(Ip->ring, smem, ring_floats);
     if (i == 0) Ip->step = s_end;
+}
+
+// Edge-parallel kernel (ring in shared memory; Linear or SigmoidalJansenRit,
+// whose pre() depends on the source region only).  Each step, thread t
+// gathers edges [t*E, t*E + E) of the row-major edge list (E <= MAXE and
+// E <= the smallest non-zero row degree, so the range covers at most two
+// rows) into two partial sums; after one barrier, thread i < n adds the
+// partials that cover row i and advances region i.  Partials are double
+// buffered by step parity, so the next step's gather can start while other
+// threads still read this step's partials; the ring needs no extra barrier
+// when every delay is >= 1 (reads stop at time s - 1 - d_min), else a second
+// barrier per step is taken.
+template <class M, int CF, int SCHEME, int MAXE>
+__global__ void __launch_bounds__(512) sim_kernel_ep(const tvbk_launch L) {
+    constexpr int NCV = M::NCV;
+    constexpr int NACC = (CF == CF_SIGMOIDAL_JR) ? 1 : NCV;
+    extern __shared__ __align__(16) float smem[];
+
+    tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x;
+    const int n = Ip->n;
+    const int t = threadIdx.x;
+    const int T = blockDim.x;
+    const bool act = t < n;
+    const int RL = Ip->ring_len;
+    const int slot_floats = n * NCV;
+    const int ring_floats = RL * slot_floats;
+    const int64_t s0 = Ip->step;
+    const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
+    if (s0 >= s_end) return;  // uniform over the block
+    const int nsteps = (int)(s_end - s0);
+    float* ring = smem;
+    float* part = smem + ((ring_floats + 3) & ~3);  // [2][T][2][NACC]
+    stage_ring(smem, Ip->ring, ring_floats);
+
+    const int nnz = Ip->nnz;
+    const int E = (nnz + T - 1) / T;
+    if (E > MAXE) {
+        if (t == 0) atomicOr(L.status + blockIdx.x, TVBK_STATUS_DEGREE);
+        return;  // uniform over the block
+    }
+    // this thread's edges: two weight sets split at kb (start of the second row)
+    const int eb = t * E;
+    const int cnt = max(0, min(E, nnz - eb));
+    int kb = MAXE;
+    if (cnt > 0) {
+        int lo = 0, hi = n - 1;  // largest r with row_ptr[r] <= eb
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(Ip->row_ptr + mid) <= eb) lo = mid; else hi = mid - 1;
+        }
+        kb = min(__ldg(Ip->row_ptr + lo + 1) - eb, cnt);
+    }
+    int off[MAXE];
+    float wa[MAXE], wb[MAXE];
+    const int2* ed2 = reinterpret_cast<const int2*>(Ip->edges) + eb;
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+        const int2 ed = (k < cnt) ? __ldg(ed2 + k) : make_int2(0, 0);
+        off[k] = ed.x;
+        const float w = __int_as_float(ed.y);
+        wa[k] = (k < kb) ? w : 0.0f;
+        wb[k] = (k < kb) ? 0.0f : w;
+    }
+    // which partials make up row t
+    int tf = -1, sf = 0, tl = -1;
+    Node<M, SCHEME> node;
+    float cf[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cf[k] = Ip->cfun[k];
+    if (act) {
+        const int e0 = Ip->row_ptr[t], e1 = Ip->row_ptr[t + 1];
+        if (e1 > e0) {
+            tf = e0 / E;
+            sf = (e0 == tf * E) ? 0 : 1;
+            tl = (e1 - 1) / E;
+        }
+        node.init(L, Ip, t, n, s0);
+    }
+    __syncthreads();
+
+    const bool zero_delay = L.sync_every <= 1;
+    int wslot = (int)(s0 % RL);
+    int par = 0;
+    for (int ks = 0; ks < nsteps; ++ks) {
+        if (act && STOCH_BLOCK_START(ks)) node.noise_block(L, t, s0 + 1 + ks);
+        const int base_off = wslot * slot_floats;  // time s - 1
+        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
+        float pa[NACC], pb[NACC];
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) pa[k] = pb[k] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < MAXE; ++k) {
+            const float* src = ring + gather_addr(base_off, off[k], ring_floats);
+            if constexpr (CF == CF_SIGMOIDAL_JR) {
+                const float2 v = *reinterpret_cast<const float2*>(src);
+                const float pre = cf[0] + (cf[1] - cf[0]) / (1.0f + expf(cf[3] * (cf[2] - (v.x - v.y))));
+                pa[0] = fmaf(wa[k], pre, pa[0]);
+                pb[0] = fmaf(wb[k], pre, pb[0]);
+            } else if constexpr (NCV == 1) {
+                const float v = src[0];
+                pa[0] = fmaf(wa[k], v, pa[0]);
+                pb[0] = fmaf(wb[k], v, pb[0]);
+            } else {
+                const float2 v = *reinterpret_cast<const float2*>(src);
+                pa[0] = fmaf(wa[k], v.x, pa[0]);
+                pa[1] = fmaf(wa[k], v.y, pa[1]);
+                pb[0] = fmaf(wb[k], v.x, pb[0]);
+                pb[1] = fmaf(wb[k], v.y, pb[1]);
+            }
+        }
+        float* pp = part + ((size_t)par * T + t) * 2 * NACC;
+#pragma unroll
+        for (int k = 0; k < NACC; ++k) {
+            pp[k] = pa[k];
+            pp[NACC + k] = pb[k];
+        }
+        __syncthreads();
+        if (act) {
+            float acc[NCV];
+#pragma unroll
+            for (int k = 0; k < NCV; ++k) acc[k] = 0.0f;
+            if (tf >= 0) {
+                const float* base = part + (size_t)par * T * 2 * NACC;
+#pragma unroll
+                for (int k = 0; k < NACC; ++k) acc[k] = base[(tf * 2 + sf) * NACC + k];
+                for (int u = tf + 1; u <= tl; ++u) {
+#pragma unroll
+                    for (int k = 0; k < NACC; ++k) acc[k] += base[u * 2 * NACC + k];
+                }
+            }
+            float c[NCV];
+            post<CF, NCV>(acc, cf, c);
+            node.advance(L, Ip, t, n, s0, ks, c);
+            node.write_ring(ring + wslot * slot_floats + t * NCV);
+        }
+        if (zero_delay) __syncthreads();
+        par ^= 1;
+    }
+    __syncthreads();
+    if (act) node.finish(L, Ip, t, n, L.status + blockIdx.x);
+    stage_ring(Ip->ring, smem, ring_floats);
+    if (t == 0) Ip->step = s_end;
 }
 
 // ------------------------------------------------------------------ launch
 
-template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD>
+template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE = false>
 int launch_one(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
-    auto kern = sim_kernel<M, CF, SCHEME, SMEM, MAXT, MAXD>;
+    auto kern = sim_kernel<M, CF, SCHEME, SMEM, MAXT, MAXD, PIPE>;
     if (smem_bytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
         if (e != cudaSuccess) return (int)e;
@@ -412,13 +602,45 @@ int launch_one(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
 // max_deg: the largest row degree over all instances of the launch.
 template <class M, int CF, int SCHEME, bool SMEM, int MAXT>
 int launch_deg(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes, int max_deg) {
+    if (max_deg <= 0) return launch_one<M, CF, SCHEME, SMEM, MAXT, 0>(L, st, smem_bytes);
+    if constexpr (CF != CF_DIFFERENCE) {
+        if (L.prefetch) {
+            if (max_deg <= 32) return launch_one<M, CF, SCHEME, SMEM, MAXT, 32, true>(L, st, smem_bytes);
+            if (max_deg <= 64) return launch_one<M, CF, SCHEME, SMEM, MAXT, 64, true>(L, st, smem_bytes);
+        }
+    }
     if (max_deg <= 32) return launch_one<M, CF, SCHEME, SMEM, MAXT, 32>(L, st, smem_bytes);
     if (max_deg <= 64) return launch_one<M, CF, SCHEME, SMEM, MAXT, 64>(L, st, smem_bytes);
     return launch_one<M, CF, SCHEME, SMEM, MAXT, 0>(L, st, smem_bytes);
 }
 
+template <class M, int CF, int SCHEME, int MAXE>
+int launch_ep(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
+    auto kern = sim_kernel_ep<M, CF, SCHEME, MAXE>;
+    if (smem_bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+        if (e != cudaSuccess) return (int)e;
+    }
+    kern<<<L.n_inst, L.block_threads, smem_bytes, st>>>(L);
+    return (int)cudaGetLastError();
+}
+
 template <class M, int CF, int SCHEME>
 int launch_scheme(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes, int max_deg) {
+    if (L.edges_per_thread > 0) {
+        if constexpr (CF == CF_DIFFERENCE) {
+            return -2;
+        } else {
+            if (!L.ring_in_smem) return -2;
+            switch (L.edges_per_thread) {
+                case 8: return launch_ep<M, CF, SCHEME, 8>(L, st, smem_bytes);
+                case 12: return launch_ep<M, CF, SCHEME, 12>(L, st, smem_bytes);
+                case 16: return launch_ep<M, CF, SCHEME, 16>(L, st, smem_bytes);
+                case 24: return launch_ep<M, CF, SCHEME, 24>(L, st, smem_bytes);
+                default: return -2;
+            }
+        }
+    }
     if (L.ring_in_smem) {
         if (L.max_n > 256) return -1;
         return launch_deg<M, CF, SCHEME, true, 256>(L, st, smem_bytes, max_deg);

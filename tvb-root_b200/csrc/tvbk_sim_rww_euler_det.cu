@@ -1,0 +1,14 @@
+// Simulation kernel instantiations for RWW with scheme TVBK_SCHEME_EULER_DET.
+#include "tvbk_sim_lanes.cuh"
+
+namespace tvbk {
+
+int launch_rww_euler_det(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
+    switch (L.cfun) {
+        case CF_LINEAR: return launch_all_scheme<RWW, CF_LINEAR, TVBK_SCHEME_EULER_DET>(L, st, smem_bytes);
+        case CF_DIFFERENCE: return launch_all_scheme<RWW, CF_DIFFERENCE, TVBK_SCHEME_EULER_DET>(L, st, smem_bytes);
+        default: return -2;
+    }
+}
+
+}  // namespace tvbk

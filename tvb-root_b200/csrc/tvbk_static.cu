@@ -153,6 +153,7 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
     L2.insts = desc;
     L2.status = status;
     L2.n_inst = 1;
+    L2.lanes = 1;
     L2.max_n = inst->n;
     L2.max_ring_len = inst->ring_len;
     L2.max_steps = inst->step_end - inst->step;

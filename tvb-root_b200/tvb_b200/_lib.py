@@ -87,6 +87,10 @@ class Launch(ctypes.Structure):
         ('sync_every', ctypes.c_int32),
         ('ring_in_smem', ctypes.c_int32),
         ('max_degree', ctypes.c_int32),
+        ('edges_per_thread', ctypes.c_int32),
+        ('block_threads', ctypes.c_int32),
+        ('prefetch', ctypes.c_int32),
+        ('lanes', ctypes.c_int32),
         ('max_steps', ctypes.c_int64),
         ('dt', ctypes.c_float),
     ]

@@ -109,7 +109,7 @@ class InstanceSpec:
 
 class Batch:
     def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
-                 sync_every=None, ring_in_smem=None):
+                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1):
         self.lib = _lib.load()
         self.device = torch.device(device if device is not None else 'cuda')
         self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
@@ -129,18 +129,92 @@ class Batch:
         if self.max_n > _lib.MAX_REGIONS:
             raise ValueError('%d regions exceed this build (%d)' % (self.max_n, _lib.MAX_REGIONS))
         hmax = max(s.conn.horizon for s in self.specs)
+        self.lanes = self._choose_lanes(lanes, gather)
+        V = self.lanes
         # stage rings in shared memory when the largest fits, shrinking K if that makes it fit
-        smem_ok = self.max_n <= 256
+        smem_ok = self.max_n <= 256 and V == 1
         if ring_in_smem is None:
             ring_in_smem = smem_ok
         if ring_in_smem:
-            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar, hmax + K) == 0:
+            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar * V, hmax + K) == 0:
                 K -= 1
-            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar, hmax + K) == 0:
+            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar * V, hmax + K) == 0:
                 ring_in_smem = False
+                K = dmin + 1 if sync_every is None else max(1, min(int(sync_every), dmin + 1))
         self.sync_every = K
         self.ring_in_smem = bool(ring_in_smem)
+        self.edges_per_thread, self.block_threads = 0, 0
+        self.prefetch = 0
+        if gather not in ('auto', 'row', 'edge'):
+            raise ValueError("gather must be 'auto', 'row' or 'edge'")
+        if gather != 'edge' and dmin >= 1 and self.cfun_id != _lib.CFUN_IDS['Difference'] \
+                and self.model_id != _lib.MODEL_IDS['Sum']:
+            # row kernel with the next step's gather issued ahead: barrier interval K <= d_min
+            self.prefetch = 1
+            self.sync_every = min(self.sync_every, dmin)
+        if gather == 'edge' and V == 1:
+            ep = self._choose_edge_parallel(dmin, hmax)
+            if ep is not None:
+                self.edges_per_thread, self.block_threads, self.sync_every = ep
+            elif gather == 'edge':
+                raise ValueError('the edge-parallel gather does not apply to this batch')
         self._build()
+
+    def _choose_lanes(self, lanes, gather):
+        """Instance groups: G = 8 / ncvar consecutive instances that share the
+        connectome object, start step and length (a parameter sweep) run
+        together, one thread per (region, instance), rings interleaved."""
+        if lanes in (None, 1, '1'):
+            return 1
+        G = 8 // self.ncvar
+        if lanes not in ('auto', G):
+            raise ValueError('instance groups have 8 / ncvar = %d lanes' % G)
+        specs = self.specs
+        same = all(s.conn is specs[0].conn and s.step0 == specs[0].step0 and s.n_steps == specs[0].n_steps
+                   for s in specs)
+        threads = -(-self.max_n * G // 32) * 32
+        smem = -(-self.max_n * self.max_degree * 8 // 16) * 16 + 2 * self.max_degree * self.ncvar * threads * 4
+        ok = (same and gather != 'edge' and self.model_id != _lib.MODEL_IDS['Sum'] and threads <= 1024
+              and smem <= 227 * 1024 and len(specs) % G == 0)
+        if ok:
+            return G
+        if lanes != 'auto':
+            raise ValueError('these instances cannot run as groups of %d' % G)
+        return 1
+
+    EP_SLOTS = (8, 12, 16, 24)
+
+    def _choose_edge_parallel(self, dmin, hmax):
+        """(edges per thread, CTA threads, barrier interval) of the edge-parallel
+        gather, or None: needs rings in shared memory, a coupling whose pre()
+        depends on the source only, and ceil(nnz / threads) <= the smallest
+        non-zero row degree.  Picks the fewest padded edge slots, then the
+        most threads."""
+        if not self.ring_in_smem or self.cfun_id == _lib.CFUN_IDS['Difference']:
+            return None
+        K = 2 if dmin >= 1 else 1
+        nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
+        need = []
+        for s in self.specs:
+            c = s.conn
+            if c.nnz == 0:
+                return None
+            deg = np.diff(c.row_ptr)
+            need.append((c.nnz, int(deg[deg > 0].min())))
+        best = None
+        for T in range(((self.max_n + 31) // 32) * 32, 513, 32):
+            ring = ((hmax + K) * self.max_n * self.ncvar + 3) // 4 * 4
+            if (ring + 2 * T * 2 * nacc) * 4 > 227 * 1024:
+                break
+            for E in self.EP_SLOTS:
+                if all(-(-nnz // T) <= min(E, mdeg) for nnz, mdeg in need):
+                    key = (T * E, -T)
+                    if best is None or key < best[0]:
+                        best = (key, E, T)
+                    break
+        if best is None:
+            return None
+        return best[1], best[2], K
 
     # ------------------------------------------------------------------ build
     def _build(self):
@@ -159,7 +233,9 @@ class Batch:
             n = s.conn.n
             RL = s.conn.horizon + self.sync_every
             m = dict(n=n, ring_len=RL)
-            init.add(('ring', k), RL * n * self.ncvar * 4)
+            V = self.lanes
+            if k % V == 0:
+                init.add(('ring', k), V * RL * n * self.ncvar * 4)
             init.add(('state', k), self.nsv * n * 4)
             init.add(('params', k), max(self.nparam, 1) * n * 4)
             if s.sigma is not None:
@@ -227,8 +303,14 @@ class Batch:
             n, RL = m['n'], m['ring_len']
             d = insts[k]
             d['row_ptr'], d['edges'] = cptr[id(s.conn)]
-            ring = ring_from_reference(s.ring0, s.step0, RL)
-            d['ring'] = put(('ring', k), ring)
+            V = self.lanes
+            if V == 1:
+                d['ring'] = put(('ring', k), ring_from_reference(s.ring0, s.step0, RL))
+            elif k % V == 0:
+                group = [ring_from_reference(specs[k + v].ring0, specs[k + v].step0, RL) for v in range(V)]
+                d['ring'] = put(('ring', k), np.stack(group, axis=-1))  # [RL][n][ncvar][V]
+            else:
+                d['ring'] = insts[k - k % V]['ring']
             d['state'] = put(('state', k), np.asarray(s.state0, dtype=np.float32))
             params = np.asarray(s.params, dtype=np.float32)
             if params.size == 0:
@@ -314,6 +396,10 @@ class Batch:
         L.sync_every = self.sync_every
         L.ring_in_smem = 1 if self.ring_in_smem else 0
         L.max_degree = self.max_degree
+        L.edges_per_thread = self.edges_per_thread
+        L.block_threads = self.block_threads
+        L.lanes = self.lanes
+        L.prefetch = self.prefetch
         L.max_steps = int(max_steps)
         L.dt = self.dt
         return L
@@ -401,7 +487,10 @@ class Batch:
 
     def ring(self, k):
         m = self.meta[k]
-        return self._iview(('ring', k), torch.float32, (m['ring_len'], m['n'], self.ncvar)).cpu().numpy()
+        V = self.lanes
+        lead = k - k % V
+        r = self._iview(('ring', lead), torch.float32, (m['ring_len'], m['n'], self.ncvar, V)).cpu().numpy()
+        return np.ascontiguousarray(r[..., k % V])
 
     def current_step(self, k):
         off, _ = self.init.regions[('insts',)]
@@ -411,6 +500,8 @@ class Batch:
     def gather_delayed(self, k, step):
         """Delayed values the coupling of `step` reads for every edge of instance k
         (read through the same address arithmetic as the kernel)."""
+        if self.lanes != 1:
+            raise ValueError('gather_delayed reads single-instance rings')
         m = self.meta[k]
         conn = self.specs[k].conn
         out = torch.empty(max(conn.nnz, 1) * self.ncvar, dtype=torch.float32, device=self.device)

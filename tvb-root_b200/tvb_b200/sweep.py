@@ -32,7 +32,8 @@ class ParameterSweep:
     """
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
-                 noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None):
+                 noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
+                 gather='auto', lanes=1):
         self.model = adopt_model(model)
         self.connectivity = adopt_connectivity(connectivity)
         self.coupling = adopt_coupling(coupling)
@@ -49,6 +50,8 @@ class ParameterSweep:
         self.device = device
         self.sync_every = sync_every
         self.ring_in_smem = ring_in_smem
+        self.gather = gather
+        self.lanes = lanes
         self.batch = None
 
     def configure(self):
@@ -105,7 +108,7 @@ class ParameterSweep:
         sim = self._sim
         self.batch = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
                            sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
-                           ring_in_smem=self.ring_in_smem)
+                           ring_in_smem=self.ring_in_smem, gather=self.gather, lanes=self.lanes)
         if self._fed is not None:
             fed = self._fed.to(self.batch.device).contiguous()
             self.batch._fed.append(fed)
