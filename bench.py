@@ -153,6 +153,116 @@ def cpu_baseline(n_steps=20000, cores=None):
                       % (cores, n_steps, n_steps * DT), 'wall_s': wall}
 
 
+# ------------------------------------------------------------ plain form
+
+def plain_form(n_steps, rank, gather):
+    """The plain single-instance form: one instance of the same sweep (one
+    CTA) through the same kernel and API, device-timed; region-steps/s."""
+    import torch
+    sw = make_sweep(1, n_steps * DT, rank=rank, gather=gather).configure()
+    b = sw.build()
+    b.snapshot()
+    st = torch.cuda.current_stream()
+    times = []
+    for k in range(4):
+        b.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sw.run_device()
+        e1.record(st)
+        torch.cuda.synchronize()
+        if k:
+            times.append(e0.elapsed_time(e1) / 1e3)
+    t = float(np.median(times))
+    return {'value': N_REGIONS * sw.n_steps / t, 'unit': UNIT, 'instances': 1, 'steps': sw.n_steps,
+            'ms': 1e3 * t}
+
+
+# ------------------------------------------------------------------ serving
+
+# per connectome size: density, tract-length range (mm), conduction speed (mm/ms), generator seed
+SERVE_SIZES = {68: (0.30, 10.0, 200.0, 5.0, 3), 76: (0.40, 10.0, 200.0, 3.0, 1), 192: (0.25, 5.0, 250.0, 4.0, 2),
+               998: (0.10, 5.0, 300.0, 3.0, 4)}
+
+
+def serving_plan(n_req, rate, seed=5):
+    """Poisson arrivals at `rate` requests/s; each request draws a connectome
+    size, a model, a duration uniform in 1-60 s and dt in {0.05, 0.1} ms."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    plan = []
+    for k in range(n_req):
+        plan.append((float(t[k]), str(rng.choice(['G2D', 'JR', 'RWW'])), int(rng.choice(list(SERVE_SIZES))),
+                     float(rng.choice([0.05, 0.1])), float(rng.uniform(1000.0, 60000.0))))
+    return plan
+
+
+def serving_sim(model, n, dt, length, seed):
+    from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.simulator import Simulator
+    dens, lo, hi, speed, cseed = SERVE_SIZES[n]
+    w, L = synthetic.connectome(n, dens, lo, hi, seed=cseed)
+    conn = Connectivity(w, L, speed=speed)
+    if model == 'G2D':
+        np.random.seed(seed)
+        return Simulator(model=models.Generic2dOscillator(), connectivity=conn, coupling=coupling.Linear(a=0.0152),
+                         integrator=integrators.HeunDeterministic(dt=dt),
+                         monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=length).configure()
+    if model == 'RWW':
+        return Simulator(model=models.ReducedWongWang(), connectivity=conn, coupling=coupling.Linear(a=0.1),
+                         integrator=integrators.EulerStochastic(dt=dt, noise=noise.Additive(nsig=[1e-3],
+                                                                                            noise_seed=seed)),
+                         monitors=[monitors.Bold(period=2000.0)], simulation_length=length).configure()
+    nsig = np.array([0.0, 0.0, 0.0, 0.0, 1e-5, 0.0])
+    return Simulator(model=models.JansenRit(), connectivity=conn, coupling=coupling.SigmoidalJansenRit(),
+                     integrator=integrators.HeunStochastic(dt=dt, noise=noise.Additive(nsig=nsig, noise_seed=seed)),
+                     monitors=[monitors.TemporalAverage(period=1.0), monitors.Bold(period=2000.0)],
+                     simulation_length=length).configure()
+
+
+def run_serving(args, rank, local):
+    """Serve a Poisson stream of simulation requests (continuous batching) and
+    print sims/s with p50/p99 latency (arrival to result on the host)."""
+    import torch
+    from tvb_b200.serving import SimulationServer
+    torch.cuda.set_device(local)
+    plan = serving_plan(args.requests, args.rate)
+    sims = [serving_sim(m, n, dt, length, seed=1000 + k) for k, (_, m, n, dt, length) in enumerate(plan)]
+    srv = SimulationServer(chunk_steps=args.chunk or 4000, device=torch.device('cuda', local))
+    arrivals = [(t, (lambda server, s=s: server.submit(s))) for (t, *_), s in zip(plan, sims)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    srv.run(arrivals=arrivals, timeout=1800.0)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    st = srv.stats()
+    bad = sum(1 for r in srv.requests.values() if r.status)
+    line = {'metric': 'serving sims/s with p50/p99 latency (continuous batching)', 'value': st['sims_per_s'],
+            'unit': 'sims/s', 'n_gpus': 1, 'steps': args.requests, 'warmup': 0, 'ms_per_step': 1e3 * wall / args.requests,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'serving_poisson', 'requests': args.requests, 'rate_per_s': args.rate,
+                       'sizes': sorted(SERVE_SIZES), 'models': ['G2D', 'JR', 'RWW'], 'duration_ms': [1000, 60000],
+                       'dt_ms': [0.05, 0.1], 'chunk_steps': srv.chunk_steps, 'state': 'f32'},
+            'latency_p50_s': st['latency_p50_s'], 'latency_p99_s': st['latency_p99_s'],
+            'latency_mean_s': st['latency_mean_s'], 'region_steps_per_s': st['region_steps_per_s'],
+            'memory_budget_bytes': st['memory_budget_bytes'], 'memory_peak_bytes': st['memory_peak_bytes'],
+            'memory_mean_bytes': st['memory_mean_bytes'], 'groups': st['groups'], 'gpu_launches': st['launches'],
+            'nonfinite_requests': bad, 'wall_s': wall}
+    if clocks:
+        line['clocks'] = clocks
+    print(json.dumps(line), flush=True)
+
+
+# DRAM bytes per instance-step of the simulation kernel on this workload, from the ncu capture
+# of 296 instances x 40 000 steps (dram__bytes_read.sum + dram__bytes_write.sum = 1.817 GB;
+# profiles/sim_kernel_rww_sweep_296i_4s.md); a launch's traffic scales with its instance-steps.
+NCU_DRAM_BYTES_PER_INSTANCE_STEP = 1.817e9 / (296 * 40000)
+
+
 # --------------------------------------------------------------------- main
 
 def run_reference(args, rank):
@@ -186,6 +296,11 @@ def main():
     ap.add_argument('--lanes', default='1', choices=['auto', '1', '2', '4', '8'],
                     help='instance groups (interleaved rings, one thread per region and instance) or one '
                          'instance per CTA')
+    ap.add_argument('--plain-steps', type=int, default=60000,
+                    help='steps of the plain single-instance measurement (0 skips it)')
+    ap.add_argument('--workload', default='sweep', choices=['sweep', 'serving'])
+    ap.add_argument('--requests', type=int, default=48, help='serving: number of requests')
+    ap.add_argument('--rate', type=float, default=4.0, help='serving: Poisson arrival rate (requests/s)')
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -193,6 +308,10 @@ def main():
     local = int(os.environ.get('LOCAL_RANK', '0'))
     if args.impl == 'reference':
         return run_reference(args, rank)
+    if args.workload == 'serving':
+        if rank == 0:
+            run_serving(args, rank, local)
+        return
 
     # CPU baseline first: its spawn pool starts before any GPU work
     cb = None
@@ -266,6 +385,8 @@ def main():
 
     if not e2e_times:
         e2e_times = [float('inf')]
+    plain = plain_form(args.plain_steps, rank, args.gather) if args.plain_steps > 0 else None
+
     if world > 1:
         tt = torch.tensor([t_dev, t_kern, float(np.median(e2e_times))], device='cuda', dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -302,9 +423,12 @@ def main():
             'e2e': {'value': region_steps / t_e2e, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d),
                     'd2h_bytes_per_step': int(d2h)},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': None,
+                         'frac': achieved / peak,
+                         'traffic': NCU_DRAM_BYTES_PER_INSTANCE_STEP * args.instances * n_steps,
                          'note': 'algorithmic gather bytes 4*ncvar*nnz per instance-step over the simulation '
-                                 'kernel time; peak = measured HBM copy bandwidth'},
+                                 'kernel time; peak = measured HBM copy bandwidth (of measured); traffic = ncu '
+                                 'DRAM bytes per launch, scaled from a 296-instance x 40 000-step capture; the '
+                                 'rings are staged in shared memory, so DRAM carries only staging and Bold'},
             'gpu_launches': launches_per_step * args.steps,
             'kernel_ms_per_step': 1e3 * t_kern,
             'nonfinite_instances': int((status != 0).sum()),
@@ -312,6 +436,9 @@ def main():
         }
         if clocks:
             line['clocks'] = clocks
+        if plain:
+            plain['batched_over_plain'] = value / plain['value']
+            line['plain_single_instance'] = plain
         if cb:
             line['cpu_baseline'] = cb
         print(json.dumps(line), flush=True)

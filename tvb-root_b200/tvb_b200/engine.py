@@ -109,7 +109,7 @@ class InstanceSpec:
 
 class Batch:
     def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
-                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1):
+                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True):
         self.lib = _lib.load()
         self.device = torch.device(device if device is not None else 'cuda')
         self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
@@ -158,7 +158,22 @@ class Batch:
                 self.edges_per_thread, self.block_threads, self.sync_every = ep
             elif gather == 'edge':
                 raise ValueError('the edge-parallel gather does not apply to this batch')
-        self._build()
+        self._plan()
+        self.allocated = False
+        if allocate:
+            self.allocate()
+
+    def allocate(self):
+        """Allocate the device arenas and upload the inputs (once)."""
+        if not self.allocated:
+            self._build()
+            self.allocated = True
+        return self
+
+    @property
+    def nbytes(self):
+        """Device bytes of this batch's arenas (inputs, accumulators, outputs)."""
+        return self.init.size + self.zero.size + self.out.size
 
     def _choose_lanes(self, lanes, gather):
         """Instance groups: G = 8 / ncvar consecutive instances that share the
@@ -217,7 +232,8 @@ class Batch:
         return best[1], best[2], K
 
     # ------------------------------------------------------------------ build
-    def _build(self):
+    def _plan(self):
+        """Arena layout and per-instance metadata (no device memory)."""
         specs, nvoi = self.specs, self.nvoi
         init, zero, outa = _Arena(), _Arena(), _Arena()
         conns = {}
@@ -265,13 +281,18 @@ class Batch:
             self.meta.append(m)
         init.add(('insts',), len(specs) * _lib.INST_DTYPE.itemsize)
         zero.add(('status',), len(specs) * 4)
+        self.init, self.zero, self.out = init, zero, outa
+        self._conns, self._hrfs = conns, hrfs
 
+    def _build(self):
+        specs = self.specs
+        init, zero, outa = self.init, self.zero, self.out
+        conns, hrfs = self._conns, self._hrfs
         dev = self.device
         self.init_buf = torch.empty(max(init.size, 1), dtype=torch.uint8, device=dev)
         self.zero_buf = torch.zeros(max(zero.size, 1), dtype=torch.uint8, device=dev)
         self.out_buf = torch.zeros(max(outa.size, 1), dtype=torch.uint8, device=dev)
         ib, zb, ob = self.init_buf.data_ptr(), self.zero_buf.data_ptr(), self.out_buf.data_ptr()
-        self.init, self.zero, self.out = init, zero, outa
 
         stage = np.zeros(max(init.size, 1), dtype=np.uint8)
 
@@ -448,7 +469,10 @@ class Batch:
 
     def outputs_host(self):
         """All outputs of all instances as numpy arrays, from one device-to-host copy."""
-        host = self.out_buf.cpu().numpy()
+        return self.outputs_from_bytes(self.out_buf.cpu().numpy())
+
+    def outputs_from_bytes(self, host):
+        """Per-instance output arrays from a host copy (uint8 array) of the output arena."""
         res = []
         for k, m in enumerate(self.meta):
             o = {}

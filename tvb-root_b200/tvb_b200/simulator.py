@@ -236,7 +236,10 @@ class Simulator:
                          k1v0=b.k1_V0)
         return raw, (tavg[0].istep if tavg else 0), bspec
 
-    def _run_device(self, n_steps):
+    def instance_spec(self, n_steps, stream=None):
+        """The device description of the next `n_steps` of this simulation and
+        its noise kind: (InstanceSpec, noise kind).  `stream` overrides the
+        Philox stream id (default: the simulator's stream_id)."""
         n = self.number_of_nodes
         raw, tavg_istep, bspec = self._monitor_spec()
         fed = None
@@ -250,9 +253,14 @@ class Simulator:
         spec = InstanceSpec(self._conn, self.history_buffer[..., 0], self.current_state[..., 0], self._params,
                             self.coupling.kernel_params(), n_steps, step0=self.current_step, sigma=self._sigma,
                             noise_fed=fed, seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
-                            stream=self.stream_id, raw=raw, tavg_istep=tavg_istep, bold=bspec)
+                            stream=self.stream_id if stream is None else stream, raw=raw, tavg_istep=tavg_istep,
+                            bold=bspec)
         if self._acc is not None:
             spec.acc0 = self._acc
+        return spec, noise_kind
+
+    def _run_device(self, n_steps):
+        spec, noise_kind = self.instance_spec(n_steps)
         batch = Batch(self._model_id, self._cfun_id, self._scheme_id, noise_kind, self.integrator.dt,
                       self._voi_codes, [spec], device=self.device)
         batch.run(chunk=self.chunk_steps)
