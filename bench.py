@@ -257,6 +257,53 @@ def run_serving(args, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------- large network
+
+def run_large_network(args, rank, local):
+    """Epileptor, 998 regions (10 % density, tract lengths 5-300 mm, speed
+    3 mm/ms), Difference coupling, HeunDeterministic dt 0.05 ms, 16 instances
+    with x0 uniform in [-2.4, -1.6] per region and uneven lengths of 2-20 s
+    in one launch, TemporalAverage 1 ms; region-steps/s of the device run."""
+    import torch
+    from tvb_b200 import coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.sweep import ParameterSweep
+    torch.cuda.set_device(local)
+    w, L = synthetic.connectome(998, 0.10, 5.0, 300.0, seed=4)
+    rng = np.random.default_rng(14 + rank)
+    x0 = rng.uniform(-2.4, -1.6, (16, 998))
+    lengths = np.linspace(2000.0, 20000.0, 16) * (args.length / 60000.0)
+    np.random.seed(15 + rank)
+    sw = ParameterSweep(model=models.Epileptor(), connectivity=Connectivity(w, L, speed=3.0),
+                        coupling=coupling.Difference(), integrator=integrators.HeunDeterministic(dt=0.05),
+                        monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=float(lengths.max()),
+                        sweep={'model.x0': x0, 'simulation_length': lengths}, gather=args.gather,
+                        cluster=args.cluster if args.cluster == 'auto' else int(args.cluster)).configure()
+    b = sw.build()
+    b.snapshot()
+    st = torch.cuda.current_stream()
+    ms = []
+    for k in range(args.warmup + args.steps):
+        b.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sw.run_device()
+        e1.record(st)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+    steps = sw.n_steps_each.sum()
+    t = float(np.mean(ms)) / 1e3
+    line = {'metric': 'region-steps/sec, large-network batch', 'value': float(steps * 998 / t), 'unit': UNIT,
+            'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'epileptor_998r_16i_uneven_2-20s', 'instances': 16, 'regions': 998,
+                       'nnz': int(sw._sim._conn.nnz), 'dt_ms': 0.05, 'lengths_ms': lengths.tolist(),
+                       'cluster_ctas_per_instance': b.cluster, 'sync_every': b.sync_every},
+            'nonfinite_instances': int((b.status() != 0).sum()), 'gpu_launches': args.steps}
+    print(json.dumps(line), flush=True)
+
+
 # DRAM bytes per instance-step of the simulation kernel on this workload, from the ncu capture
 # of 296 instances x 40 000 steps (dram__bytes_read.sum + dram__bytes_write.sum = 1.817 GB;
 # profiles/sim_kernel_rww_sweep_296i_4s.md); a launch's traffic scales with its instance-steps.
@@ -298,7 +345,8 @@ def main():
                          'instance per CTA')
     ap.add_argument('--plain-steps', type=int, default=60000,
                     help='steps of the plain single-instance measurement (0 skips it)')
-    ap.add_argument('--workload', default='sweep', choices=['sweep', 'serving'])
+    ap.add_argument('--workload', default='sweep', choices=['sweep', 'serving', 'large-network'])
+    ap.add_argument('--cluster', default='auto', help='CTAs per instance (large-network workload)')
     ap.add_argument('--requests', type=int, default=48, help='serving: number of requests')
     ap.add_argument('--rate', type=float, default=4.0, help='serving: Poisson arrival rate (requests/s)')
     args = ap.parse_args()
@@ -311,6 +359,10 @@ def main():
     if args.workload == 'serving':
         if rank == 0:
             run_serving(args, rank, local)
+        return
+    if args.workload == 'large-network':
+        if rank == 0:
+            run_large_network(args, rank, local)
         return
 
     # CPU baseline first: its spawn pool starts before any GPU work

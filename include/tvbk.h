@@ -103,6 +103,9 @@ typedef struct tvbk_inst {
     const tvbk_edge* edges;      /* [nnz] packed offsets and weights (tvbk_pack_edges) */
     /* dynamic state */
     float* ring;                 /* [ring_len][n][ncvar] */
+    float* pre_ring;             /* [ring_len][n] SigmoidalJansenRit with the row or cluster kernel and rings
+                                  * read in place: the gather ring of pre-applied sigmoid values (scratch,
+                                  * recomputed from `ring` at every launch); NULL otherwise */
     float* state;                /* [nsv][n] */
     /* parameters */
     const float* params;         /* [nparam][n] model parameters, one value per region */
@@ -154,6 +157,11 @@ typedef struct tvbk_launch {
                                   * read in place (regions * lanes <= 1024 threads; the edge list and two
                                   * staging buffers of max_degree * ncvar floats per thread must fit in
                                   * shared memory) */
+    int32_t cluster;             /* 0 or 1: one CTA per instance; 2..16: a thread-block cluster of that many CTAs
+                                  * per instance, each owning ceil(max_n / cluster) <= 480 rows, rings read in
+                                  * place (lanes 1, row gather, rings not in shared memory) */
+    int32_t cluster_edges;       /* cluster kernel: edges of one CTA's rows that it stages in shared memory; a CTA
+                                  * with more edges reads them from global memory (0: always global) */
     int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */
     float dt;
 } tvbk_launch;
@@ -197,7 +205,14 @@ int tvbk_model_dims(int32_t model, int32_t* ncvar, int32_t* nsv, int32_t* nintva
 
 /* Run up to L->max_steps steps of every instance (one CTA per instance).
  * Coupling parameters in tvbk_inst.cfun: Linear {a, b}; Difference {a};
- * SigmoidalJansenRit {cmin, cmax, midpoint, r, a}. */
+ * SigmoidalJansenRit {cmin, cmax, midpoint, r, a}.  SigmoidalJansenRit's
+ * pre() depends on the source region only: the row kernel (lanes 1,
+ * edges_per_thread 0) and the cluster kernel apply it once per region and
+ * step and gather from a ring of those values, one float per (slot, region),
+ * so their edges are packed with ncvar = 1 (tvbk_pack_edges) and, with rings
+ * read in place, each instance needs a pre_ring; the edge-parallel and
+ * instance-group kernels apply it per edge and use edges packed with
+ * ncvar = 2. */
 int tvbk_sim_run(const tvbk_launch* L, void* stream);
 
 /* Delayed-state gather of one instance at step `step` (the values the

@@ -174,6 +174,36 @@ def test_epileptor_998_difference():
     assert rms <= 1e-2
 
 
+def test_epileptor_998_batch_uneven_lengths():
+    """Large-network batch: Epileptor, 998 regions, Difference coupling,
+    HeunDeterministic dt 0.05, x0 uniform in [-2.4, -1.6] per region and per
+    instance, uneven lengths in one launch (a thread-block cluster per
+    instance); every instance against the float64-state oracle, error
+    reported per instance."""
+    from tvb_b200 import coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.sweep import ParameterSweep
+    w, L = synthetic.connectome(998, 0.10, 5.0, 300.0, seed=4)
+    rng = np.random.default_rng(12)
+    x0 = rng.uniform(-2.4, -1.6, (4, 998))
+    lengths = np.array([5.0, 10.0, 15.0, 20.0])
+    np.random.seed(13)
+    sw = ParameterSweep(model=models.Epileptor(), connectivity=Connectivity(w, L, speed=3.0),
+                        coupling=coupling.Difference(), integrator=integrators.HeunDeterministic(dt=0.05),
+                        monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=20.0,
+                        sweep={'model.x0': x0, 'simulation_length': lengths}).configure()
+    buf0 = sw._sim.history_buffer[..., 0].copy()
+    st0 = sw._sim.current_state[..., 0].copy()
+    res = sw.run(fc=False)
+    assert sw.batch.cluster >= 2 and (res['status'] == 0).all()
+    for i in range(4):
+        n_steps = int(round(lengths[i] / 0.05))
+        out, _ = O.simulate('Epileptor', {'x0': x0[i]}, w, L, 3.0, 0.05, 'Difference', {'a': 0.1},
+                            'HeunDeterministic', n_steps, [O.Monitor('TemporalAverage', 1.0)], buf0, st0, 0)
+        assert res['tavg'][i].shape == out[0][1].shape
+        report('epileptor 998 batch instance %d (%g ms) tavg' % (i, lengths[i]), res['tavg'][i], out[0][1], 1e-4)
+
+
 def test_jansen_rit_sigmoidal_heun_stochastic_reference_noise():
     """JR + SigmoidalJansenRit + HeunStochastic over the full 4000 ms with the
     reference's own noise stream; TemporalAverage and Bold."""
@@ -268,9 +298,10 @@ def test_philox_stream_matches_oracle():
 
 @pytest.mark.parametrize('cfun', ['Linear', 'SigmoidalJansenRit', 'Difference'])
 def test_kernel_variants_agree(cfun):
-    """The row kernel, the edge-parallel kernel (balanced edge split, row
-    partials) and the instance-lane kernels (2 and 4 interleaved instances,
-    rings in shared or global memory) compute the same trajectories up to
+    """The row kernel (rings in shared or global memory), the edge-parallel
+    kernel (balanced edge split, row partials), the instance-lane kernels (2
+    and 4 interleaved instances) and the cluster kernel (4 and 16 CTAs per
+    instance, warp-per-row gather) compute the same trajectories up to
     float32 summation order."""
     import bench
     from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
@@ -301,24 +332,44 @@ def test_kernel_variants_agree(cfun):
         sweep = {'coupling.a': np.linspace(0.5, 2.0, 8)}
         mons, length = [monitors.TemporalAverage(period=1.0)], 200.0
     out = {}
-    variants = [('row', 1, None), ('row', 1, False), ('row', 'auto', None)]
+    variants = [('row', 1, None, 0), ('row', 1, False, 0), ('row', 'auto', None, 0), ('row', 1, False, 4),
+                ('row', 1, False, 16)]
     if cfun != 'Difference':
-        variants.append(('edge', 1, None))
-    for gather, lanes, smem in variants:
+        variants.append(('edge', 1, None, 0))
+    for gather, lanes, smem, cluster in variants:
         np.random.seed(11)
         sw = ParameterSweep(model=model, connectivity=Connectivity(w, L, speed=5.0), coupling=cf, integrator=integ(),
                             monitors=mons, simulation_length=length, sweep=sweep, gather=gather, lanes=lanes,
-                            ring_in_smem=smem).configure()
+                            ring_in_smem=smem, cluster=cluster).configure()
         res = sw.run(fc=False)
         assert (res['status'] == 0).all()
-        key = (gather, sw.batch.lanes, sw.batch.ring_in_smem)
+        key = (gather, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster)
         if lanes == 'auto':
             assert sw.batch.lanes == 8 // sw.batch.ncvar
         if gather == 'edge':
             assert sw.batch.edges_per_thread > 0
+        assert sw.batch.cluster == cluster
         out[key] = res
-    base = out[('row', 1, True)]
+    base = out[('row', 1, True, 0)]
     for key, res in out.items():
         for mon in ('tavg', 'bold'):
-            if mon in res and key != ('row', 1, True):
+            if mon in res and key != ('row', 1, True, 0):
                 report('%s %s %s vs row' % (cfun, mon, key), res[mon], base[mon], 1e-5)
+
+
+def test_chunked_graph_replay_matches_one_launch():
+    """Chunked launches replayed from a CUDA graph (the kernel continues from
+    each instance's device-side step) give bit-identical outputs to one launch
+    over all steps and to eager chunked launches."""
+    import bench
+    outs = {}
+    for label, chunk, graph in (('one', None, False), ('eager', 700, False), ('graph', 700, True)):
+        sw = bench.make_sweep(16, 5000.0, chunk=chunk).configure()
+        sw.build()
+        sw.run_device(graph=graph)
+        outs[label] = np.stack([o['bold'] for o in sw.batch.outputs_host()])
+        assert (sw.batch.status() == 0).all()
+        if graph:
+            assert sw.batch._graph_launches >= 2
+    np.testing.assert_array_equal(outs['eager'], outs['one'])
+    np.testing.assert_array_equal(outs['graph'], outs['one'])

@@ -201,6 +201,25 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
     if (stoch && L->noise != TVBK_NOISE_FED && L->noise != TVBK_NOISE_PHILOX)
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: stochastic scheme needs fed or Philox noise");
     if (L->max_steps == 0) return TVBK_OK;
+    if (L->cluster < 0 || L->cluster > 16)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster %d out of 0..16", L->cluster);
+    if (L->cluster > 1) {
+        if (L->lanes > 1 || L->edges_per_thread != 0 || L->ring_in_smem)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster per instance uses the row gather with rings in "
+                        "place (lanes 1, edges_per_thread 0, ring_in_smem 0)");
+        if (L->model == TVBK_MODEL_SUM) return fail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run: clusters with the Sum model");
+        const int64_t R = ((int64_t)L->max_n + L->cluster - 1) / L->cluster;
+        if (R > 480)
+            return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: %lld rows per cluster CTA, at most 480 (use a larger cluster)",
+                        (long long)R);
+        if (L->cluster_edges < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster_edges < 0");
+        const int64_t nacc = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
+        const int64_t b = ((R + 1) * 4 + 15) / 16 * 16 + (2 * R * nacc * 4 + 15) / 16 * 16 +
+                          (int64_t)L->cluster_edges * 8;
+        if (b > kMaxSmemPerBlock)
+            return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: cluster CTA needs %lld bytes of shared memory",
+                        (long long)b);
+    }
     size_t smem = 0;
     if (L->lanes > 1) {
         if (L->lanes * d.ncvar != 8)
@@ -239,7 +258,9 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         smem = (size_t)b;
     } else if (L->ring_in_smem) {
         if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
-        const int64_t b = (int64_t)L->max_ring_len * L->max_n * d.ncvar * (int64_t)sizeof(float);
+        // the row kernel stages one pre-applied sigmoid value per (slot, region) for SigmoidalJansenRit
+        const int64_t ncv_g = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
+        const int64_t b = (int64_t)L->max_ring_len * L->max_n * ncv_g * (int64_t)sizeof(float);
         if (b > kMaxSmemPerBlock || L->max_n > 256)
             return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: ring of %lld bytes / %d regions cannot be staged in "
                         "shared memory", (long long)b, L->max_n);

@@ -1,0 +1,273 @@
+// Cluster variant of the simulation kernel for large instances.
+//
+// One instance is advanced by a thread-block cluster of C CTAs (C = the
+// launch's `cluster`, 2..16).  CTA r of the cluster owns the rows (target
+// regions) [r*R, min(n, r*R + R)), R = ceil(n / C): it keeps those rows'
+// edges in shared memory, computes their coupling sums, and advances their
+// regions.  The history ring stays in global memory (L2 / HBM) and is read
+// with L2-coherent loads (ld.global.cg).
+//
+// Per step, within a CTA:
+//   * gather warps: one warp per row at a time -- the 32 lanes take the
+//     row's edges strided by 32 (coalesced edge reads, independent ring
+//     loads), accumulate w * pre(x_i, x_j(t - d)) and reduce with warp
+//     shuffles; rows are taken four at a time so that up to 4 * MAXE loads
+//     per lane are in flight.  The sums go to a shared buffer, double
+//     buffered by step parity.
+//   * update warps (the first ceil(R / 32); thread t advances row r*R + t):
+//     post(), the scheme step with noise, the ring write and the monitors --
+//     the same per-region code as the single-CTA kernel.
+// For SigmoidalJansenRit the gather reads a ring of pre-applied sigmoid
+// values (GatherTraits), recomputed from the raw ring at the start of a launch
+// and written beside it every step.
+// With PIPE (every delay >= 1 and barrier interval K <= d_min), the gather
+// warps compute the sums of step s + 1 while the update warps advance step
+// s: that gather reads times <= s - d_min only.  Without it every warp
+// gathers, then the update warps advance, in the same step.
+//
+// Across the cluster, ring writes become visible to the other CTAs at a
+// cluster barrier (arrive.release / wait.acquire) every K steps.  Within a
+// window of K <= d_min (PIPE) or K <= d_min + 1 steps no CTA reads a time
+// written in the window, and ring_len >= horizon + K keeps every write of
+// the window off slots still to be read, as in the single-CTA kernel.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "tvbk_sim_impl.cuh"
+
+namespace tvbk {
+
+namespace cgx = cooperative_groups;
+
+constexpr int kClusterThreads = 512;
+constexpr int kClusterRowsPerPass = 4;
+
+__host__ __device__ inline int cluster_rows(int n, int C) { return (n + C - 1) / C; }
+
+// Shared memory of one cluster CTA: row pointers, the double-buffered sums
+// and (when they fit) the CTA's edges.
+__host__ __device__ inline size_t cluster_smem_head(int R, int nacc) {
+    return ((size_t)(R + 1) * 4 + 15) / 16 * 16 + ((size_t)2 * R * nacc * 4 + 15) / 16 * 16;
+}
+
+template <int NCV>
+__device__ __forceinline__ void load_cg(const float* p, float* v) {
+    if constexpr (NCV == 1) {
+        v[0] = __ldcg(p);
+    } else {
+        const float2 t = __ldcg(reinterpret_cast<const float2*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+    }
+}
+
+template <int CF, int NCV, int NACC>
+__device__ __forceinline__ void accumulate_v(float* acc, float w, const float* v, const float* xi, const float* cf) {
+    if constexpr (CF == CF_SIGMOIDAL_JR) {
+        const float pre = cf[0] + (cf[1] - cf[0]) / (1.0f + expf(cf[3] * (cf[2] - (v[0] - v[1]))));
+        acc[0] = fmaf(w, pre, acc[0]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < NCV; ++q) acc[q] = fmaf(w, (CF == CF_DIFFERENCE) ? v[q] - xi[q] : v[q], acc[q]);
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class M, int CF, int SCHEME, int MAXE, bool PIPE>
+__global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const tvbk_launch L) {
+    constexpr int NCV = M::NCV;
+    constexpr int NACC = (CF == CF_SIGMOIDAL_JR) ? 1 : NCV;
+    constexpr bool SIGMA = GatherTraits<CF, NCV>::SIGMA;
+    constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
+    constexpr int RP = kClusterRowsPerPass;
+    extern __shared__ __align__(16) unsigned char sm[];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x / C;
+    int32_t* status = L.status + blockIdx.x / C;
+    const int n = Ip->n;
+    const int R = cluster_rows(n, C);
+    const int r0 = min(n, rank * R), r1 = min(n, r0 + R), nr = r1 - r0;
+    const int RL = Ip->ring_len;
+    const int slot_floats = n * NG;  // the gather ring: NG floats per (slot, region)
+    const int ring_floats = RL * slot_floats;
+    const int64_t s0 = Ip->step;
+    const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
+    if (s0 >= s_end) return;  // uniform over the cluster
+    const int nsteps = (int)(s_end - s0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, W = blockDim.x >> 5;
+
+    int* rp = reinterpret_cast<int*>(sm);
+    float* csum = reinterpret_cast<float*>(sm + ((size_t)(R + 1) * 4 + 15) / 16 * 16);
+    int2* esm = reinterpret_cast<int2*>(sm + cluster_smem_head(R, NACC));
+    const int e_lo = Ip->row_ptr[r0], e_hi = Ip->row_ptr[r1];
+    const int ne = e_hi - e_lo;
+    const int2* eg = reinterpret_cast<const int2*>(Ip->edges) + e_lo;
+    // the CTA's edges in shared memory when they fit the launch's allowance, else read from global
+    const bool e_in_smem = ne <= L.cluster_edges;
+    const int2* ed = e_in_smem ? esm : eg;
+    for (int k = tid; k <= nr; k += blockDim.x) rp[k] = Ip->row_ptr[r0 + k] - e_lo;
+    if (e_in_smem)
+        for (int k = tid; k < ne; k += blockDim.x) esm[k] = __ldg(eg + k);
+
+    float cf[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cf[k] = Ip->cfun[k];
+    const int U = (nr + 31) >> 5;                  // update warps
+    const int G0 = PIPE ? U : 0;                   // first gather warp
+    const int G = PIPE ? W - U : W;                // gather warps
+    const bool upd = tid < nr;
+    Node<M, SCHEME> node;
+    if (upd) {
+        node.init(L, Ip, r0 + tid, n, s0);
+        if (Ip->row_ptr[r0 + tid + 1] - Ip->row_ptr[r0 + tid] > 32 * MAXE) atomicOr(status, TVBK_STATUS_DEGREE);
+    }
+    float* __restrict__ raw = Ip->ring;
+    // gather ring: the raw ring, or for SigmoidalJansenRit the pre-applied sigmoid values, recomputed from
+    // the raw ring at every launch (split over the cluster, visible to all of it after the cluster barrier)
+    float* __restrict__ ring = SIGMA ? Ip->pre_ring : raw;
+    if constexpr (SIGMA) {
+        sigma_ring(ring, raw, RL * n, rank * blockDim.x + tid, C * blockDim.x, cf);
+        cluster.sync();
+    } else {
+        __syncthreads();
+    }
+
+    // coupling sums of the step whose time s - 1 is in slot `prev`, into csum[buf]
+    auto gather = [&](int prev, int buf) {
+        const int base_off = prev * slot_floats;
+        float* out = csum + (size_t)buf * R * NACC;
+        for (int first = warp - G0; first < nr; first += G * RP) {
+            float acc[RP][NACC];
+#pragma unroll
+            for (int h = 0; h < RP; ++h) {
+#pragma unroll
+                for (int q = 0; q < NACC; ++q) acc[h][q] = 0.0f;
+                const int lr = first + h * G;
+                if (lr < nr) {  // uniform over the warp
+                    float xi[NCV];
+                    if constexpr (CF == CF_DIFFERENCE) load_cg<NCV>(ring + base_off + (r0 + lr) * NCV, xi);
+                    const int eb = rp[lr], ee = rp[lr + 1];
+#pragma unroll
+                    for (int k = 0; k < MAXE; ++k) {
+                        const int e = eb + lane + 32 * k;
+                        if (e < ee) {
+                            const int2 p = ed[e];
+                            float v[NG];
+                            load_cg<NG>(ring + gather_addr(base_off, p.x, ring_floats), v);
+                            accumulate_v<GCF, NG, NACC>(acc[h], __int_as_float(p.y), v, xi, cf);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < RP; ++h) {
+                const int lr = first + h * G;
+                if (lr < nr) {
+#pragma unroll
+                    for (int q = 0; q < NACC; ++q) {
+                        const float t = warp_sum(acc[h][q]);
+                        if (lane == 0) out[lr * NACC + q] = t;
+                    }
+                }
+            }
+        }
+    };
+    auto update = [&](int ks, int wslot, int buf) {
+        const float* in = csum + (size_t)buf * R * NACC;
+        float a[NACC], c[NCV];
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) a[q] = in[tid * NACC + q];
+        post<CF, NCV>(a, cf, c);
+        if (STOCH_BLOCK_START(ks)) node.noise_block(L, r0 + tid, s0 + 1 + ks);
+        node.advance(L, Ip, r0 + tid, n, s0, ks, c);
+        node.write_ring(raw + (size_t)wslot * n * NCV + (r0 + tid) * NCV);
+        if constexpr (SIGMA)
+            ring[wslot * slot_floats + r0 + tid] = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+    };
+
+    const int K = L.sync_every;
+    int since_sync = 0;
+    int wslot = (int)(s0 % RL);  // slot of the last written time
+    if constexpr (PIPE) {
+        if (warp >= G0) gather(wslot, 0);
+        __syncthreads();
+    }
+    for (int ks = 0; ks < nsteps; ++ks) {
+        const int prev = wslot;
+        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
+        if constexpr (PIPE) {
+            if (warp < U) {
+                if (upd) update(ks, wslot, ks & 1);
+            } else if (ks + 1 < nsteps) {
+                gather(wslot, (ks + 1) & 1);  // step s + 1: times <= s - d_min
+            }
+            __syncthreads();
+        } else {
+            gather(prev, 0);
+            __syncthreads();
+            if (upd) update(ks, wslot, 0);
+            __syncthreads();
+        }
+        if (++since_sync == K) {
+            since_sync = 0;
+            cluster.sync();
+        }
+    }
+    cluster.sync();
+    if (upd) node.finish(L, Ip, r0 + tid, n, status);
+    if (rank == 0 && tid == 0) Ip->step = s_end;
+}
+
+template <class M, int CF, int SCHEME, int MAXE, bool PIPE>
+int launch_cluster_t(const tvbk_launch& L, cudaStream_t st) {
+    auto kern = sim_kernel_cluster<M, CF, SCHEME, MAXE, PIPE>;
+    constexpr int NACC = (CF == CF_SIGMOIDAL_JR) ? 1 : M::NCV;
+    const int C = L.cluster;
+    const int R = cluster_rows(L.max_n, C);
+    const size_t smem = cluster_smem_head(R, NACC) + (size_t)L.cluster_edges * 8;
+    if (smem > 227 * 1024) return -1;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    if (C > 8) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return (int)e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(L.n_inst * C), 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, kern, L);
+    return (int)e;
+}
+
+template <class M, int CF, int SCHEME, bool PIPE>
+int launch_cluster_p(const tvbk_launch& L, cudaStream_t st) {
+    if (L.max_degree <= 64) return launch_cluster_t<M, CF, SCHEME, 2, PIPE>(L, st);
+    if (L.max_degree <= 128) return launch_cluster_t<M, CF, SCHEME, 4, PIPE>(L, st);
+    if (L.max_degree <= 256) return launch_cluster_t<M, CF, SCHEME, 8, PIPE>(L, st);
+    if (L.max_degree <= 1024) return launch_cluster_t<M, CF, SCHEME, 32, PIPE>(L, st);
+    return -1;
+}
+
+template <class M, int CF, int SCHEME>
+int launch_cluster(const tvbk_launch& L, cudaStream_t st) {
+    if (L.prefetch) return launch_cluster_p<M, CF, SCHEME, true>(L, st);
+    return launch_cluster_p<M, CF, SCHEME, false>(L, st);
+}
+
+}  // namespace tvbk

@@ -79,6 +79,35 @@ __device__ __forceinline__ void post(const float* acc, const float* cf, float* c
     }
 }
 
+// SigmoidalJansenRit's pre() depends on the source region's delayed state
+// only, so the row and cluster kernels apply it once per (time, region), when
+// the state is written, and keep a gather ring of those values (one float per
+// slot and region): the same float32 expression on the same operands as
+// applying it per edge, with one exp per region-step instead of one per edge.
+// The ring of raw coupling variables is still written every step (it is the
+// history the caller reads back).  GatherTraits gives the gather's view: the
+// number of floats per (slot, region) it reads and the coupling it applies.
+template <int CF, int NCV>
+struct GatherTraits {
+    static constexpr bool SIGMA = (CF == CF_SIGMOIDAL_JR);
+    static constexpr int NG = SIGMA ? 1 : NCV;
+    static constexpr int GCF = SIGMA ? CF_LINEAR : CF;
+};
+
+__device__ __forceinline__ float sjr_pre(float v0, float v1, const float* cf) {
+    return cf[0] + (cf[1] - cf[0]) / (1.0f + expf(cf[3] * (cf[2] - (v0 - v1))));
+}
+
+// Fill a gather ring of pre-applied sigmoid values from the raw ring
+// [nslots*n][2]: elements [k0, nelem) strided by `stride`.
+__device__ __forceinline__ void sigma_ring(float* dst, const float* __restrict__ raw, int nelem, int k0, int stride,
+                                           const float* cf) {
+    for (int k = k0; k < nelem; k += stride) {
+        const float2 v = reinterpret_cast<const float2*>(raw)[k];
+        dst[k] = sjr_pre(v.x, v.y, cf);
+    }
+}
+
 // Row gather with edges in registers: two partial sums (even / odd edges).
 // The loop is branch-free so that every shared-memory load can be issued
 // ahead of its use: padding slots (k >= deg) carry weight 0 and offset 0,
@@ -105,18 +134,19 @@ struct RegRow {
     __device__ __forceinline__ void couple(const float* __restrict__ ring, int base_off, int ring_floats,
                                            const float* xi, const float* cf, float* c) const {
         constexpr int NCV = M::NCV;
-        float a0[NCV], a1[NCV];
+        constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
+        float a0[NG], a1[NG];
 #pragma unroll
-        for (int k = 0; k < NCV; ++k) a0[k] = a1[k] = 0.0f;
+        for (int k = 0; k < NG; ++k) a0[k] = a1[k] = 0.0f;
         const char* rb = reinterpret_cast<const char*>(ring);
         const int base_b = base_off * (int)sizeof(float), ring_b = ring_floats * (int)sizeof(float);
 #pragma unroll
         for (int k = 0; k < MAXD; ++k) {
             const int a = gather_addr(base_b, off[k], ring_b);
-            accumulate<CF, NCV>((k & 1) ? a1 : a0, w[k], reinterpret_cast<const float*>(rb + a), xi, cf);
+            accumulate<GCF, NG>((k & 1) ? a1 : a0, w[k], reinterpret_cast<const float*>(rb + a), xi, cf);
         }
 #pragma unroll
-        for (int k = 0; k < NCV; ++k) a0[k] += a1[k];
+        for (int k = 0; k < NG; ++k) a0[k] += a1[k];
         post<CF, NCV>(a0, cf, c);
     }
 };
@@ -135,21 +165,22 @@ struct RegRow<M, CF, 0> {
     __device__ __forceinline__ void couple(const float* __restrict__ ring, int base_off, int ring_floats,
                                            const float* xi, const float* cf, float* c) const {
         constexpr int NCV = M::NCV;
-        float a0[NCV], a1[NCV];
+        constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
+        float a0[NG], a1[NG];
 #pragma unroll
-        for (int k = 0; k < NCV; ++k) a0[k] = a1[k] = 0.0f;
+        for (int k = 0; k < NG; ++k) a0[k] = a1[k] = 0.0f;
         int e = 0;
         for (; e + 1 < deg; e += 2) {
             const int2 p = __ldg(ed2 + e), q = __ldg(ed2 + e + 1);
-            accumulate<CF, NCV>(a0, __int_as_float(p.y), ring + gather_addr(base_off, p.x, ring_floats), xi, cf);
-            accumulate<CF, NCV>(a1, __int_as_float(q.y), ring + gather_addr(base_off, q.x, ring_floats), xi, cf);
+            accumulate<GCF, NG>(a0, __int_as_float(p.y), ring + gather_addr(base_off, p.x, ring_floats), xi, cf);
+            accumulate<GCF, NG>(a1, __int_as_float(q.y), ring + gather_addr(base_off, q.x, ring_floats), xi, cf);
         }
         if (e < deg) {
             const int2 p = __ldg(ed2 + e);
-            accumulate<CF, NCV>(a0, __int_as_float(p.y), ring + gather_addr(base_off, p.x, ring_floats), xi, cf);
+            accumulate<GCF, NG>(a0, __int_as_float(p.y), ring + gather_addr(base_off, p.x, ring_floats), xi, cf);
         }
 #pragma unroll
-        for (int k = 0; k < NCV; ++k) a0[k] += a1[k];
+        for (int k = 0; k < NG; ++k) a0[k] += a1[k];
         post<CF, NCV>(a0, cf, c);
     }
 };
@@ -376,6 +407,8 @@ __device__ __forceinline__ void stage_ring(float* dst, const float* src, int nfl
 template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE>
 __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     constexpr int NCV = M::NCV;
+    constexpr bool SIGMA = GatherTraits<CF, NCV>::SIGMA;
+    constexpr int NG = GatherTraits<CF, NCV>::NG;
     extern __shared__ __align__(16) float smem[];
 
     tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x;
@@ -383,21 +416,26 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     const int i = threadIdx.x;
     const bool act = i < n;
     const int RL = Ip->ring_len;
-    const int slot_floats = n * NCV;
+    const int slot_floats = n * NG;             // the gather ring: NG floats per (slot, region)
     const int ring_floats = RL * slot_floats;
     const int64_t s0 = Ip->step;
     const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
     if (s0 >= s_end) return;  // uniform over the block
     const int nsteps = (int)(s_end - s0);
 
-    float* ring = SMEM ? smem : Ip->ring;
-    if (SMEM) {
-        stage_ring(smem, Ip->ring, ring_floats);
-        __syncthreads();
-    }
     float cf[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) cf[k] = Ip->cfun[k];
+    // gather ring: the raw ring (staged in shared memory or in place), or for
+    // SigmoidalJansenRit the pre-applied sigmoid values computed from it
+    float* ring = SMEM ? smem : (SIGMA ? Ip->pre_ring : Ip->ring);
+    if constexpr (SIGMA) {
+        sigma_ring(ring, Ip->ring, RL * n, threadIdx.x, blockDim.x, cf);
+        __syncthreads();
+    } else if (SMEM) {
+        stage_ring(smem, Ip->ring, ring_floats);
+        __syncthreads();
+    }
     RegRow<M, CF, MAXD> row;
     row.deg = 0;
     Node<M, SCHEME> node;
@@ -430,7 +468,12 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                 row.couple(ring, prev * slot_floats, ring_floats, xi, cf, c);
             }
             node.advance(L, Ip, i, n, s0, ks, c);
-            node.write_ring(ring + wslot * slot_floats + i * NCV);
+            if constexpr (SIGMA) {
+                node.write_ring(Ip->ring + (size_t)wslot * n * NCV + i * NCV);  // raw history
+                ring[wslot * slot_floats + i] = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+            } else {
+                node.write_ring(ring + wslot * slot_floats + i * NCV);
+            }
         }
         if (++since_sync == K) {
             since_sync = 0;
@@ -439,7 +482,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     }
     __syncthreads();
     if (act) node.finish(L, Ip, i, n, L.status + blockIdx.x);
-    if (SMEM) stage_ring(Ip->ring, smem, ring_floats);
+    if (SMEM && !SIGMA) stage_ring(Ip->ring, smem, ring_floats);
     if (i == 0) Ip->step = s_end;
 }
 

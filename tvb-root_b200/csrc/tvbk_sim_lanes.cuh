@@ -15,6 +15,7 @@
 #pragma once
 #include <cuda_pipeline.h>
 
+#include "tvbk_sim_cluster.cuh"
 #include "tvbk_sim_impl.cuh"
 
 namespace tvbk {
@@ -218,11 +219,12 @@ int launch_group(const tvbk_launch& L, cudaStream_t st, int max_deg) {
     return launch_group_one<M, CF, SCHEME, G, false>(L, st);
 }
 
-// Dispatch on the launch's variant for one scheme: instance groups, else the
-// row / edge-parallel kernels.
+// Dispatch on the launch's variant for one scheme: instance groups, clusters
+// of CTAs per instance, else the row / edge-parallel kernels.
 template <class M, int CF, int SCHEME>
 int launch_all_scheme(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
     if (L.lanes > 1) return launch_group<M, CF, SCHEME>(L, st, L.max_degree);
+    if (L.cluster > 1) return launch_cluster<M, CF, SCHEME>(L, st);
     return launch_scheme<M, CF, SCHEME>(L, st, smem_bytes, L.max_degree);
 }
 

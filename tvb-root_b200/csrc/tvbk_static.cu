@@ -90,7 +90,7 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
         return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: ring_len %d < horizon + sync_every", inst->ring_len);
     if (inst->step_end < inst->step) return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: step_end < step");
 
-    // scratch layout: descriptor | status | tavg_acc | bold_acc | bold_stock | ring
+    // scratch layout: descriptor | status | tavg_acc | bold_acc | bold_stock | ring | pre_ring
     const int64_t n = inst->n, nvoi = L->nvoi;
     const bool tavg = inst->tavg != nullptr, bold = inst->bold != nullptr;
     if (bold && (!inst->hrf || inst->stock_len <= 0))
@@ -111,6 +111,10 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
     const size_t o_ring = off;
     const int64_t ring_floats = (int64_t)inst->ring_len * n * ncvar;
     off = align256(off + (size_t)ring_floats * sizeof(float));
+    // SigmoidalJansenRit: the kernel's ring of pre-applied sigmoid values (filled by the kernel itself)
+    const bool pre = L->cfun == TVBK_CFUN_SIGMOIDAL_JR;
+    const size_t o_pre = off;
+    off = align256(off + (pre ? (size_t)inst->ring_len * n * sizeof(float) : 0));
     if (off > (size_t)TVBK_STATIC_SCRATCH_BYTES)
         return sfail(TVBK_ERR_TOO_LARGE,
                      "tvbk_sim_run_static: needs %zu bytes of scratch (ring %lld floats%s), the library holds %d",
@@ -135,6 +139,7 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
 
     tvbk_inst d = *inst;
     d.ring = reinterpret_cast<float*>(base + o_ring);
+    d.pre_ring = pre ? reinterpret_cast<float*>(base + o_pre) : nullptr;
     d.tavg_acc = tavg ? reinterpret_cast<float*>(base + o_tacc) : nullptr;
     d.bold_acc = bold ? reinterpret_cast<double*>(base + o_bacc) : nullptr;
     d.bold_stock = bold ? reinterpret_cast<double*>(base + o_stock) : nullptr;

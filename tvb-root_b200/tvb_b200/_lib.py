@@ -39,6 +39,7 @@ class Inst(ctypes.Structure):
         ('row_ptr', ctypes.c_void_p),
         ('edges', ctypes.c_void_p),
         ('ring', ctypes.c_void_p),
+        ('pre_ring', ctypes.c_void_p),
         ('state', ctypes.c_void_p),
         ('params', ctypes.c_void_p),
         ('noise_sigma', ctypes.c_void_p),
@@ -91,6 +92,8 @@ class Launch(ctypes.Structure):
         ('block_threads', ctypes.c_int32),
         ('prefetch', ctypes.c_int32),
         ('lanes', ctypes.c_int32),
+        ('cluster', ctypes.c_int32),
+        ('cluster_edges', ctypes.c_int32),
         ('max_steps', ctypes.c_int64),
         ('dt', ctypes.c_float),
     ]

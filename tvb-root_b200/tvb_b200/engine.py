@@ -73,6 +73,13 @@ class Connectome:
         self.horizon = int(np.asarray(idelays).max()) + 1
         self.ncvar = ncvar
         self.edges = _lib.pack_edges(self.col, self.idelay, self.weight, self.n, ncvar)
+        self._packed = {ncvar: self.edges}
+
+    def packed(self, ncvar):
+        """Gather edges for a ring with `ncvar` floats per (slot, region)."""
+        if ncvar not in self._packed:
+            self._packed[ncvar] = _lib.pack_edges(self.col, self.idelay, self.weight, self.n, ncvar)
+        return self._packed[ncvar]
 
 
 class InstanceSpec:
@@ -109,7 +116,7 @@ class InstanceSpec:
 
 class Batch:
     def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
-                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True):
+                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True, cluster='auto'):
         self.lib = _lib.load()
         self.device = torch.device(device if device is not None else 'cuda')
         self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
@@ -131,14 +138,19 @@ class Batch:
         hmax = max(s.conn.horizon for s in self.specs)
         self.lanes = self._choose_lanes(lanes, gather)
         V = self.lanes
+        # SigmoidalJansenRit with the row / cluster kernels gathers from a ring of pre-applied sigmoid
+        # values, one float per (slot, region)
+        self.sigma = (self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] and V == 1 and gather != 'edge')
+        self.ncvar_gather = 1 if self.sigma else self.ncvar
         # stage rings in shared memory when the largest fits, shrinking K if that makes it fit
         smem_ok = self.max_n <= 256 and V == 1
+        ncg = self.ncvar if gather == 'edge' else self.ncvar_gather
         if ring_in_smem is None:
             ring_in_smem = smem_ok
         if ring_in_smem:
-            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar * V, hmax + K) == 0:
+            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, ncg * V, hmax + K) == 0:
                 K -= 1
-            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, self.ncvar * V, hmax + K) == 0:
+            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, ncg * V, hmax + K) == 0:
                 ring_in_smem = False
                 K = dmin + 1 if sync_every is None else max(1, min(int(sync_every), dmin + 1))
         self.sync_every = K
@@ -158,6 +170,7 @@ class Batch:
                 self.edges_per_thread, self.block_threads, self.sync_every = ep
             elif gather == 'edge':
                 raise ValueError('the edge-parallel gather does not apply to this batch')
+        self.cluster, self.cluster_edges = self._choose_cluster(cluster)
         self._plan()
         self.allocated = False
         if allocate:
@@ -196,6 +209,50 @@ class Batch:
         if lanes != 'auto':
             raise ValueError('these instances cannot run as groups of %d' % G)
         return 1
+
+    CLUSTER_SMEM = 227 * 1024
+    CLUSTER_MAX_ROWS = 480
+
+    def _choose_cluster(self, cluster):
+        """CTAs per instance (thread-block cluster) and the per-CTA edge
+        allowance in shared memory.  'auto', for rings read in place and at
+        least 64 regions: 16 CTAs per instance for up to 16 instances (their
+        clusters run in waves when they outnumber the SMs, which also keeps
+        each wave's rings closer to L2-sized), SMs // instances CTAs up to
+        SMs / 2 instances, else one CTA per instance."""
+        if cluster in (None, 0, 1, '0', '1'):
+            return 0, 0
+        able = (self.lanes == 1 and not self.ring_in_smem and not self.edges_per_thread
+                and self.model_id != _lib.MODEL_IDS['Sum'])
+        if cluster == 'auto':
+            if not able or self.max_n < 64:
+                return 0, 0
+            sms = 148
+            if self.device.type == 'cuda' and torch.cuda.is_available():
+                sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+            ni = len(self.specs)
+            C = 16 if ni <= 16 else sms // ni
+            C = min(C, -(-self.max_n // 4))
+            if C < 2:
+                return 0, 0
+        else:
+            C = int(cluster)
+            if not able or not 2 <= C <= 16:
+                raise ValueError('a cluster of 2..16 CTAs per instance needs rings in place, the row gather and '
+                                 'one instance per group')
+        C = max(C, -(-self.max_n // self.CLUSTER_MAX_ROWS))
+        R = -(-self.max_n // C)
+        nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
+        head = -(-(R + 1) * 4 // 16) * 16 + -(-2 * R * nacc * 4 // 16) * 16
+        emax = 0
+        for s in self.specs:
+            rp = s.conn.row_ptr
+            n = s.conn.n
+            for r in range(C):
+                lo = min(n, r * R)
+                hi = min(n, lo + R)
+                emax = max(emax, int(rp[hi] - rp[lo]))
+        return C, (emax if head + 8 * emax <= self.CLUSTER_SMEM else 0)
 
     EP_SLOTS = (8, 12, 16, 24)
 
@@ -252,6 +309,8 @@ class Batch:
             V = self.lanes
             if k % V == 0:
                 init.add(('ring', k), V * RL * n * self.ncvar * 4)
+            if self.sigma and not self.ring_in_smem:
+                zero.add(('pre_ring', k), RL * n * 4)
             init.add(('state', k), self.nsv * n * 4)
             init.add(('params', k), max(self.nparam, 1) * n * 4)
             if s.sigma is not None:
@@ -313,7 +372,7 @@ class Batch:
 
         cptr = {}
         for key, c in conns.items():
-            cptr[key] = (put(('row_ptr', key), c.row_ptr), put(('edges', key), c.edges)
+            cptr[key] = (put(('row_ptr', key), c.row_ptr), put(('edges', key), c.packed(self.ncvar_gather))
                          if c.nnz else ib + init.regions[('edges', key)][0])
         hptr = {key: put(('hrf', key), np.asarray(h, dtype=np.float64)) for key, h in hrfs.items()}
 
@@ -332,6 +391,7 @@ class Batch:
                 d['ring'] = put(('ring', k), np.stack(group, axis=-1))  # [RL][n][ncvar][V]
             else:
                 d['ring'] = insts[k - k % V]['ring']
+            d['pre_ring'] = zaddr(('pre_ring', k))
             d['state'] = put(('state', k), np.asarray(s.state0, dtype=np.float32))
             params = np.asarray(s.params, dtype=np.float32)
             if params.size == 0:
@@ -420,23 +480,58 @@ class Batch:
         L.edges_per_thread = self.edges_per_thread
         L.block_threads = self.block_threads
         L.lanes = self.lanes
+        L.cluster = self.cluster
+        L.cluster_edges = self.cluster_edges
         L.prefetch = self.prefetch
         L.max_steps = int(max_steps)
         L.dt = self.dt
         return L
 
-    def run(self, n_steps=None, chunk=None, stream=None):
+    def run(self, n_steps=None, chunk=None, stream=None, graph=False):
         """Advance every instance by up to n_steps (default: to its end) in
-        launches of at most `chunk` steps."""
+        launches of at most `chunk` steps.
+
+        graph=True: the chunk launches are recorded once into a CUDA graph of
+        up to `graph_launches` launches (the kernel reads each instance's step
+        from its device descriptor, so replaying the same launches continues
+        the run) and the graph is replayed; a remainder runs eagerly."""
         left = self.max_total - self.steps_done if n_steps is None else int(n_steps)
         chunk = left if chunk is None else int(chunk)
         st = torch.cuda.current_stream(self.device) if stream is None else stream
+        if graph and chunk > 0 and left >= 2 * chunk:
+            reps = left // chunk
+            g = self._chunk_graph(chunk, min(reps, self.graph_launches), st)
+            per = self._graph_launches
+            with torch.cuda.stream(st):
+                for _ in range(reps // per):
+                    g.replay()
+            done = (reps // per) * per * chunk
+            left -= done
+            self.steps_done += done
         while left > 0:
             k = min(chunk, left)
             L = self.launch_struct(k)
             _lib.check(self.lib.tvbk_sim_run(ctypes.byref(L), ctypes.c_void_p(st.cuda_stream)))
             left -= k
             self.steps_done += k
+
+    graph_launches = 64
+
+    def _chunk_graph(self, chunk, launches, st):
+        """CUDA graph of `launches` chunk launches of `chunk` steps (cached)."""
+        key = (chunk, launches)
+        if getattr(self, '_graph_key', None) == key:
+            return self._graph
+        L = self.launch_struct(chunk)
+        g = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(device=self.device)
+        cap.wait_stream(st)
+        with torch.cuda.graph(g, stream=cap, capture_error_mode='relaxed'):
+            for _ in range(launches):
+                _lib.check(self.lib.tvbk_sim_run(ctypes.byref(L), ctypes.c_void_p(cap.cuda_stream)))
+        st.wait_stream(cap)
+        self._graph, self._graph_key, self._graph_launches = g, key, launches
+        return g
 
     # ---------------------------------------------------------------- outputs
     def _zview(self, key, dtype, shape):
@@ -524,8 +619,8 @@ class Batch:
     def gather_delayed(self, k, step):
         """Delayed values the coupling of `step` reads for every edge of instance k
         (read through the same address arithmetic as the kernel)."""
-        if self.lanes != 1:
-            raise ValueError('gather_delayed reads single-instance rings')
+        if self.lanes != 1 or self.sigma:
+            raise ValueError('gather_delayed reads single-instance rings of raw coupling variables')
         m = self.meta[k]
         conn = self.specs[k].conn
         out = torch.empty(max(conn.nnz, 1) * self.ncvar, dtype=torch.float32, device=self.device)

@@ -203,6 +203,8 @@ class SimulationServer:
         L.max_degree = max(p.max_degree for p in plans)
         L.prefetch = 1 if all(p.prefetch for p in plans) else 0
         L.lanes = 1
+        L.cluster = p0.cluster
+        L.cluster_edges = max(p.cluster_edges for p in plans)
         L.max_steps = self.chunk_steps
         L.dt = p0.dt
         st = g.stream

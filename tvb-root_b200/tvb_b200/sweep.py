@@ -23,8 +23,12 @@ from . import monitors as monitors_mod
 class ParameterSweep:
     """Sweep of `n_instances` simulations.
 
-    sweep: dict mapping 'coupling.<name>', 'noise.nsig' or 'model.<name>' to
-    arrays of one value per instance.  Noise: 'philox' draws an independent
+    sweep: dict mapping 'coupling.<name>', 'noise.nsig', 'model.<name>' or
+    'simulation_length' to arrays of one value per instance (for
+    'model.<name>' also an (instances, regions) array: one value per region,
+    like the reference's spatialised parameters); 'simulation_length' gives
+    instances of uneven lengths, which run in the same launch and retire at
+    their own last step.  Noise: 'philox' draws an independent
     device stream per instance (key = (noise_seed, instance index));
     'reference' feeds every instance the reference's RandomState stream (the
     same for all, as separate reference runs with the default seed would
@@ -33,7 +37,7 @@ class ParameterSweep:
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
                  noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
-                 gather='auto', lanes=1):
+                 gather='auto', lanes=1, cluster='auto'):
         self.model = adopt_model(model)
         self.connectivity = adopt_connectivity(connectivity)
         self.coupling = adopt_coupling(coupling)
@@ -41,7 +45,7 @@ class ParameterSweep:
         self.monitors = [adopt_monitor(m) for m in (monitors if isinstance(monitors, (list, tuple)) else [monitors])]
         self.simulation_length = float(simulation_length)
         self.sweep = {k: np.atleast_1d(np.asarray(v, dtype=np.float64)) for k, v in sweep.items()}
-        sizes = {v.size for v in self.sweep.values()}
+        sizes = {len(v) for v in self.sweep.values()}
         if len(sizes) != 1:
             raise ValueError('all swept parameters need the same number of values')
         self.n_instances = sizes.pop()
@@ -52,6 +56,7 @@ class ParameterSweep:
         self.ring_in_smem = ring_in_smem
         self.gather = gather
         self.lanes = lanes
+        self.cluster = cluster
         self.batch = None
 
     def configure(self):
@@ -74,25 +79,33 @@ class ParameterSweep:
             fed = torch.from_numpy(z)
         self._fed = fed
         specs = []
+        lengths = self.sweep.get('simulation_length')
+        if lengths is not None:
+            self.n_steps_each = np.ceil(lengths / self.integrator.dt).astype(np.int64)
+            self.n_steps = int(self.n_steps_each.max())
+        else:
+            self.n_steps_each = np.full(self.n_instances, self.n_steps, dtype=np.int64)
         for i in range(self.n_instances):
             params = base_params
             cf = self.coupling.kernel_params()
             sigma = sim._sigma
             for key, vals in self.sweep.items():
-                part, name = key.split('.', 1)
+                part, _, name = key.partition('.')
                 if part == 'model':
                     if params is base_params:
                         params = base_params.copy()
-                    params[pidx[name]] = np.float32(vals[i])
+                    params[pidx[name]] = np.asarray(vals[i], dtype=np.float32)
                 elif part == 'coupling':
                     cf = list(cf)
                     cf[cnames.index(name)] = float(vals[i])
                 elif part == 'noise' and name == 'nsig':
                     sigma = noise_sigma(np.array([vals[i]]), sim.nint, n, self.integrator.dt)
+                elif key == 'simulation_length':
+                    pass
                 else:
                     raise ValueError('cannot sweep %s' % key)
             spec = InstanceSpec(conn, sim.history_buffer[..., 0], sim.current_state[..., 0], params, cf,
-                                self.n_steps, step0=sim.current_step, sigma=sigma, noise_fed=None,
+                                int(self.n_steps_each[i]), step0=sim.current_step, sigma=sigma, noise_fed=None,
                                 seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                                 stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec)
             specs.append(spec)
@@ -103,12 +116,28 @@ class ParameterSweep:
         self._noise_kind = noise_kind
         return self
 
-    def build(self):
-        """Allocate the device batch and upload inputs (one host-to-device copy)."""
+    def _make_batch(self, gather, lanes, ring_in_smem, cluster):
         sim = self._sim
-        self.batch = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
-                           sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
-                           ring_in_smem=self.ring_in_smem, gather=self.gather, lanes=self.lanes)
+        return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
+                     sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
+                     ring_in_smem=ring_in_smem, gather=gather, lanes=lanes, cluster=cluster)
+
+    def build(self):
+        """Allocate the device batch and upload inputs (one host-to-device copy).
+        With gather='tune' the kernel variant is picked by the autotuner
+        (trial runs of this batch, cached per GPU and batch shape)."""
+        sim = self._sim
+        kw = dict(gather=self.gather, lanes=self.lanes, ring_in_smem=self.ring_in_smem, cluster=self.cluster)
+        if self.gather == 'tune' and self._fed is not None:
+            kw['gather'] = 'auto'  # trial runs draw no fed noise: fed-noise parity runs keep the default variant
+        elif self.gather == 'tune':
+            from . import autotune
+            dev = torch.device(self.device if self.device is not None else 'cuda')
+            key = autotune.shape_key(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind,
+                                     self.integrator.dt, sim._voi_codes, self._specs, dev)
+            kw, self.tune_ms = autotune.tune(self._make_batch, key, sim.ncvar, sim.number_of_nodes,
+                                             self.n_instances, shared_conn=True)
+        self.batch = self._make_batch(**kw)
         if self._fed is not None:
             fed = self._fed.to(self.batch.device).contiguous()
             self.batch._fed.append(fed)
@@ -118,9 +147,13 @@ class ParameterSweep:
             self.batch.init_buf[off:off + ins.nbytes].copy_(torch.from_numpy(ins.view(np.uint8)))
         return self.batch
 
-    def run_device(self):
-        """Advance every instance to the end on the device (inputs already resident)."""
-        self.batch.run(chunk=self.chunk_steps)
+    def run_device(self, graph=None):
+        """Advance every instance to the end on the device (inputs already
+        resident).  With chunk_steps set, the chunk launches are replayed from
+        a CUDA graph (graph=None or True) or launched one by one (False)."""
+        if graph is None:
+            graph = self.chunk_steps is not None
+        self.batch.run(chunk=self.chunk_steps, graph=graph)
 
     def bold_device(self, voi=0):
         """(I, T, n) float64 device tensor of the Bold series of one observed variable."""
@@ -133,7 +166,8 @@ class ParameterSweep:
 
     def run(self, fc=True):
         """Build, run and return host results: dict with per-monitor arrays
-        (I, T, nvoi, n) under 'raw' / 'tavg' / 'bold' and 'fc' (I, n, n)."""
+        (I, T, nvoi, n) under 'raw' / 'tavg' / 'bold' (lists of (T_i, nvoi, n)
+        arrays for uneven lengths) and 'fc' (I, n, n)."""
         if self.batch is None:
             self.build()
         self.run_device()
@@ -143,6 +177,8 @@ class ParameterSweep:
         outs = self.batch.outputs_host()
         for key in ('raw', 'tavg', 'bold'):
             if key in outs[0]:
-                res[key] = np.stack([o[key] for o in outs])
+                arrs = [o[key] for o in outs]
+                # instances of uneven lengths give a list of (T_i, nvoi, n) arrays
+                res[key] = np.stack(arrs) if len({a.shape for a in arrs}) == 1 else arrs
         res['status'] = self.batch.status()
         return res
