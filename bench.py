@@ -338,7 +338,7 @@ def main():
     ap.add_argument('--cpu-steps', type=int, default=20000)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-steps', type=int, default=2)
-    ap.add_argument('--gather', default='auto', choices=['auto', 'row', 'edge'],
+    ap.add_argument('--gather', default='auto', choices=['auto', 'row', 'edge', 'split', 'tune'],
                     help='coupling gather variant of the simulation kernel')
     ap.add_argument('--lanes', default='1', choices=['auto', '1', '2', '4', '8'],
                     help='instance groups (interleaved rings, one thread per region and instance) or one '

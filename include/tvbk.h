@@ -149,7 +149,10 @@ typedef struct tvbk_launch {
     int32_t block_threads;       /* CTA size for the edge-parallel gather (multiple of 32, >= max_n, <= 512) */
     int32_t prefetch;            /* 1: issue the gather of step s + 1 before the update of step s (row kernel,
                                   * Linear or SigmoidalJansenRit); needs every delay >= 1 and
-                                  * 1 <= sync_every <= the smallest delay */
+                                  * 1 <= sync_every <= the smallest delay.  2: the same overlap with separate
+                                  * warps -- ceil(max_n / 32) gather warps sum the rows of step s + 1 while as
+                                  * many update warps advance step s (rings in shared memory, row degrees
+                                  * <= 64; one CTA barrier per step) */
     int32_t lanes;               /* 1, or 8 / ncvar: instance groups.  Consecutive groups of `lanes` instances
                                   * share connectome, ring length and step range; one thread advances one
                                   * (region, instance) pair and the group's rings are interleaved

@@ -298,7 +298,8 @@ def test_philox_stream_matches_oracle():
 
 @pytest.mark.parametrize('cfun', ['Linear', 'SigmoidalJansenRit', 'Difference'])
 def test_kernel_variants_agree(cfun):
-    """The row kernel (rings in shared or global memory), the edge-parallel
+    """The row kernel (rings in shared or global memory), its split form
+    (separate gather and update warps, same summation order), the edge-parallel
     kernel (balanced edge split, row partials), the instance-lane kernels (2
     and 4 interleaved instances) and the cluster kernel (4 and 16 CTAs per
     instance, warp-per-row gather) compute the same trajectories up to
@@ -335,7 +336,7 @@ def test_kernel_variants_agree(cfun):
     variants = [('row', 1, None, 0), ('row', 1, False, 0), ('row', 'auto', None, 0), ('row', 1, False, 4),
                 ('row', 1, False, 16)]
     if cfun != 'Difference':
-        variants.append(('edge', 1, None, 0))
+        variants += [('edge', 1, None, 0), ('split', 1, True, 0)]
     for gather, lanes, smem, cluster in variants:
         np.random.seed(11)
         sw = ParameterSweep(model=model, connectivity=Connectivity(w, L, speed=5.0), coupling=cf, integrator=integ(),

@@ -194,7 +194,12 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: voi %d out of range", L->voi[v]);
     if (L->sync_every < 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: sync_every must be >= 1");
     if (L->max_degree < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_degree < 0");
-    if (L->prefetch != 0 && L->prefetch != 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch must be 0 or 1");
+    if (L->prefetch < 0 || L->prefetch > 2) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch must be 0, 1 or 2");
+    if (L->prefetch == 2 && (!L->ring_in_smem || L->lanes > 1 || L->edges_per_thread != 0 || L->cluster > 1 ||
+                             L->cfun == TVBK_CFUN_DIFFERENCE || L->max_degree > 64 || L->model == TVBK_MODEL_SUM))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch 2 (separate gather warps) needs rings in shared memory, "
+                    "the row gather (lanes 1, no edge split, no cluster), Linear or SigmoidalJansenRit coupling and "
+                    "row degrees <= 64");
     if (L->max_steps < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_steps < 0");
     if (!(L->dt > 0.0f)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: dt must be > 0");
     const bool stoch = L->scheme == TVBK_SCHEME_EULER_STOCH || L->scheme == TVBK_SCHEME_HEUN_STOCH;
@@ -260,7 +265,9 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
         // the row kernel stages one pre-applied sigmoid value per (slot, region) for SigmoidalJansenRit
         const int64_t ncv_g = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
-        const int64_t b = (int64_t)L->max_ring_len * L->max_n * ncv_g * (int64_t)sizeof(float);
+        int64_t b = (int64_t)L->max_ring_len * L->max_n * ncv_g * (int64_t)sizeof(float);
+        // separate gather warps pass the sums through a double buffer after the ring
+        if (L->prefetch == 2) b = (b + 15) / 16 * 16 + (int64_t)2 * L->max_n * d.ncvar * (int64_t)sizeof(float);
         if (b > kMaxSmemPerBlock || L->max_n > 256)
             return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: ring of %lld bytes / %d regions cannot be staged in "
                         "shared memory", (long long)b, L->max_n);

@@ -13,8 +13,10 @@ namespace tvbk {
 // offset of time s - 1, edge_off = (idelay * n - col) * ncvar.  The slot of
 // time s - 1 - idelay wraps around when base_off - edge_off is negative.
 __device__ __forceinline__ int gather_addr(int base_off, int edge_off, int ring_floats) {
-    const int a = base_off - edge_off;
-    return a < 0 ? a + ring_floats : a;
+    // as unsigned, a negative base_off - edge_off is above every wrapped address:
+    // min(a, a + ring_floats) picks the in-ring one (one fused add-min)
+    const unsigned a = (unsigned)(base_off - edge_off);
+    return (int)__viaddmin_u32(a, (unsigned)ring_floats, a);
 }
 
 // Generic2dOscillator (tvb/simulator/models/oscillator.py:387-395).
@@ -22,6 +24,7 @@ __device__ __forceinline__ int gather_addr(int base_off, int edge_off, int ring_
 struct G2D {
     static constexpr int NSV = 2, NCV = 1, NINT = 2, NOBS = 4, NP = 12;
     __device__ static constexpr int cvar(int k) { return 0; }
+    __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* x, const float* c, const float* p, float* dx) {
         const float V = x[0], W = x[1];
         const float V2 = V * V;
@@ -47,6 +50,7 @@ struct G2D {
 struct JansenRit {
     static constexpr int NSV = 6, NCV = 2, NINT = 6, NOBS = 6, NP = 13;
     __device__ static constexpr int cvar(int k) { return k == 0 ? 1 : 2; }
+    __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* y, const float* c, const float* p, float* dx) {
         const float A = p[0], B = p[1], a = p[2], b = p[3], v0 = p[4], nu = p[5], r = p[6], J = p[7],
                     a1 = p[8], a2 = p[9], a3 = p[10], a4 = p[11], mu = p[12];
@@ -70,24 +74,50 @@ struct JansenRit {
     __device__ __forceinline__ static void bound(float* x) {}
 };
 
+// expm1(x) / x = sum_{k=0..12} x^k / (k+1)!, the Taylor series of expm1
+// divided by x, for |x| <= 1: the truncation (the x^13 / 14! term, below
+// 1.2e-11 relative) is far under float32 rounding.
+__device__ __forceinline__ float expm1_over_x(float x) {
+    float q = 1.0f / 6227020800.0f;  // 1 / 13!
+    q = fmaf(q, x, 1.0f / 479001600.0f);
+    q = fmaf(q, x, 1.0f / 39916800.0f);
+    q = fmaf(q, x, 1.0f / 3628800.0f);
+    q = fmaf(q, x, 1.0f / 362880.0f);
+    q = fmaf(q, x, 1.0f / 40320.0f);
+    q = fmaf(q, x, 1.0f / 5040.0f);
+    q = fmaf(q, x, 1.0f / 720.0f);
+    q = fmaf(q, x, 1.0f / 120.0f);
+    q = fmaf(q, x, 1.0f / 24.0f);
+    q = fmaf(q, x, 1.0f / 6.0f);
+    q = fmaf(q, x, 0.5f);
+    return fmaf(q, x, 1.0f);
+}
+
 // ReducedWongWang (tvb/simulator/models/wong_wang.py:36-42); S bounded to [0, 1] (wong_wang.py:129-133).
-// params: a, b, d, gamma, tau_s, w, J_N, I_o
+// params: a, b, d, gamma, tau_s, w, J_N, I_o (prepare() replaces tau_s by 1 / tau_s)
 //
-// H(x) = (a x - b) / (1 - exp(-d (a x - b))) is evaluated as -y / expm1(-d y)
-// with y = a x - b: the same function without the cancellation of 1 - exp(.)
-// near y = 0, where float32 would lose most digits; its limit 1/d is used for
-// |d y| below 1e-6.
+// H(x) = (a x - b) / (1 - exp(-d (a x - b))) = -y / expm1(-d y) with
+// y = a x - b.  For |d y| <= 1 it is 1 / (d * (expm1(-d y) / (-d y))), the
+// ratio from its series: no cancellation near y = 0 and no 0/0 at y = 0 (the
+// limit 1/d comes out of the same expression); for |d y| > 1, where
+// exp(-d y) - 1 does not cancel, -y / (exp(-d y) - 1) with the hardware
+// exponential.  Both forms are evaluated and one is selected (no branch).
 struct RWW {
     static constexpr int NSV = 1, NCV = 1, NINT = 1, NOBS = 1, NP = 8;
     __device__ static constexpr int cvar(int k) { return 0; }
+    __device__ __forceinline__ static void prepare(float* p) { p[4] = 1.0f / p[4]; }
     __device__ __forceinline__ static void dfun(const float* x, const float* c, const float* p, float* dx) {
         const float S = x[0];
-        const float a = p[0], b = p[1], d = p[2], gamma = p[3], tau_s = p[4], w = p[5], JN = p[6], Io = p[7];
+        const float a = p[0], b = p[1], d = p[2], gamma = p[3], inv_tau_s = p[4], w = p[5], JN = p[6], Io = p[7];
         const float xx = w * JN * S + Io + JN * c[0];
         const float y = a * xx - b;
         const float dy = d * y;
-        const float h = (fabsf(dy) > 1e-6f) ? (-y / expm1f(-dy)) : (1.0f / d);
-        dx[0] = -(S / tau_s) + (1.0f - S) * h * gamma;
+        const bool small = fabsf(dy) <= 1.0f;
+        const float q = expm1_over_x(small ? -dy : 0.0f);
+        const float num = small ? 1.0f : -y;
+        const float den = small ? d * q : __expf(-dy) - 1.0f;
+        const float h = num * __frcp_rn(den);
+        dx[0] = fmaf((1.0f - S) * h, gamma, -(S * inv_tau_s));
     }
     __device__ __forceinline__ static float observe(int k, const float* x) { return x[0]; }
     __device__ __forceinline__ static void bound(float* x) { x[0] = fminf(fmaxf(x[0], 0.0f), 1.0f); }
@@ -98,6 +128,7 @@ struct RWW {
 struct Epileptor {
     static constexpr int NSV = 6, NCV = 2, NINT = 6, NOBS = 7, NP = 17;
     __device__ static constexpr int cvar(int k) { return k == 0 ? 0 : 3; }
+    __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* y, const float* c, const float* p, float* dx) {
         const float a = p[0], b = p[1], cc = p[2], d = p[3], r = p[4], x0 = p[5], Iext = p[6], slope = p[7],
                     Iext2 = p[8], tau = p[9], aa = p[10], bb = p[11], Kvf = p[12], Kf = p[13], Ks = p[14],
@@ -143,6 +174,7 @@ struct Epileptor {
 struct SumModel {
     static constexpr int NSV = 1, NCV = 1, NINT = 1, NOBS = 1, NP = 1;
     __device__ static constexpr int cvar(int k) { return 0; }
+    __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* x, const float* c, const float* p, float* dx) {
         dx[0] = x[0] + c[0];
     }

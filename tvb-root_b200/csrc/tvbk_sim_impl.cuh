@@ -214,6 +214,7 @@ struct Node {
         for (int k = 0; k < NSV; ++k) x[k] = Ip->state[k * n + i];
 #pragma unroll
         for (int k = 0; k < NP; ++k) p[k] = Ip->params[k * n + i];
+        M::prepare(p);
 #pragma unroll
         for (int k = 0; k < NINT; ++k) sig[k] = STOCH ? Ip->noise_sigma[k * n + i] : 0.0f;
 #pragma unroll
@@ -257,26 +258,9 @@ struct Node {
         }
     }
 
-    // One step s = s0 + 1 + ks with coupling input c.  The caller writes the
-    // new coupling variables x[cvar(k)] to the ring.
-    __device__ __forceinline__ void advance(const tvbk_launch& L, const tvbk_inst* Ip, int i, int n, int64_t s0,
-                                            int ks, const float* c) {
-        const float dt = L.dt;
-        const int nvoi = L.nvoi;
-        float z[NINT];
-        if constexpr (STOCH) {
-            if (L.noise == TVBK_NOISE_FED) {
-#pragma unroll
-                for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
-                fed_p += (size_t)NINT * n;
-            } else {
-                const int r = (int)((s0 + 1 + ks) & 3);
-#pragma unroll
-                for (int k = 0; k < NINT; ++k)
-                    z[k] = (r == 0) ? zc[k][0] : (r == 1) ? zc[k][1] : (r == 2) ? zc[k][2] : zc[k][3];
-            }
-        }
-
+    // The scheme step with coupling input c and standard normals z (integrators.py:296-426),
+    // then the state-variable bounds.
+    __device__ __forceinline__ void integrate(const float* c, const float* z, float dt) {
         float m0[NSV];
         M::dfun(x, c, p, m0);
         if constexpr (SCHEME == TVBK_SCHEME_EULER_DET) {
@@ -303,6 +287,29 @@ struct Node {
             for (int k = 0; k < NSV; ++k) x[k] = m0[k];
         }
         M::bound(x);
+    }
+
+    // One step s = s0 + 1 + ks with coupling input c.  The caller writes the
+    // new coupling variables x[cvar(k)] to the ring.
+    __device__ __forceinline__ void advance(const tvbk_launch& L, const tvbk_inst* Ip, int i, int n, int64_t s0,
+                                            int ks, const float* c) {
+        const float dt = L.dt;
+        const int nvoi = L.nvoi;
+        float z[NINT];
+        if constexpr (STOCH) {
+            if (L.noise == TVBK_NOISE_FED) {
+#pragma unroll
+                for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
+                fed_p += (size_t)NINT * n;
+            } else {
+                const int r = (int)((s0 + 1 + ks) & 3);
+#pragma unroll
+                for (int k = 0; k < NINT; ++k)
+                    z[k] = (r == 0) ? zc[k][0] : (r == 1) ? zc[k][1] : (r == 2) ? zc[k][2] : zc[k][3];
+            }
+        }
+
+        integrate(c, z, dt);
 
         // monitors
         if (raw_p != nullptr) {
@@ -361,6 +368,133 @@ struct Node {
                 }
                 bold_p += (size_t)nvoi * n;
             }
+        }
+    }
+
+    // ---- pieces of a step for the row kernel's blocked loop ----------------
+    // Monitor clock: steps until the next TemporalAverage sample (cd_t), Bold
+    // 4 ms stock write (cd_i) and Bold TR sample (cd_b); kBigCount when the
+    // monitor is off.  It depends on the descriptor only, so every thread of
+    // the CTA (active or not) keeps the same clock and the kernel's control
+    // flow can branch on it uniformly.
+    static constexpr int kBigCount = 1 << 30;
+    int cd_t, cd_i, cd_b;
+    bool on_t, on_b;
+
+    __device__ __forceinline__ void init_clock(const tvbk_inst* Ip, int64_t s0) {
+        t_istep = Ip->tavg_istep;
+        b_istep = Ip->bold_istep;
+        b_ii = Ip->bold_ii;
+        on_t = Ip->tavg != nullptr;
+        on_b = Ip->bold != nullptr;
+        cd_t = on_t ? Ip->tavg_istep - (int)(s0 % Ip->tavg_istep) : kBigCount;
+        cd_i = on_b ? Ip->bold_ii - (int)(s0 % Ip->bold_ii) : kBigCount;
+        cd_b = on_b ? Ip->bold_istep - (int)(s0 % Ip->bold_istep) : kBigCount;
+    }
+
+    // Per-step monitor accumulation (Raw rows, TemporalAverage and Bold sums), no sampling.
+    __device__ __forceinline__ void accumulate(const tvbk_launch& L, int n) {
+        const int nvoi = L.nvoi;
+        if (raw_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) raw_p[v * n] = M::observe(L.voi[v], x);
+            raw_p += (size_t)nvoi * n;
+        }
+        if (tavg_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) tacc[v] += M::observe(L.voi[v], x);
+        }
+        if (bold_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) bacc[v] += (double)M::observe(L.voi[v], x);
+        }
+    }
+
+    // Advance the clock by m steps, the last of which is step s, and take the
+    // samples that fall on step s (every thread calls it; `act` threads write).
+    // m > 1 only when no sample falls on the m - 1 steps before s.
+    __device__ __forceinline__ void tick(int m, bool act, int64_t s, int i, int n, int nvoi) {
+        if (on_t) cd_t -= m;
+        if (cd_t == 0) {
+            cd_t = t_istep;
+            if (act) {
+                const float inv_n = (float)t_istep;
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) {
+                        tavg_p[v * n] = tacc[v] / inv_n;
+                        tacc[v] = 0.0f;
+                    }
+                tavg_p += (size_t)nvoi * n;
+            }
+        }
+        if (on_b) {
+            cd_i -= m;
+            cd_b -= m;
+        }
+        if (cd_i == 0) {
+            cd_i = b_ii;
+            if (act) {
+                double* st = stock + (size_t)q_prev * nvoi * n + i;
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) {
+                        st[v * n] = bacc[v] / (double)b_ii;
+                        bacc[v] = 0.0;
+                    }
+                q_prev = (q_prev + 1 == SL) ? 0 : q_prev + 1;
+            }
+        }
+        if (cd_b == 0) {
+            cd_b = b_istep;
+            if (act) bold_sample(s, i, n, nvoi);
+        }
+    }
+
+    // Bold output at step s: (hrf . stock - 1) k1 V0 with the kernel rolled to the current stock position.
+    __device__ __forceinline__ void bold_sample(int64_t s, int i, int n, int nvoi) {
+        const int m = (int)((s / b_ii) % SL);
+        // numpy.roll(hrf, m - 1)[k] == hrf[(k - m + 1) mod SL]
+        int idx0 = 1 - m;
+        idx0 = idx0 < 0 ? idx0 + SL : (idx0 >= SL ? idx0 - SL : idx0);
+        for (int v = 0; v < nvoi; ++v) {
+            double dot = 0.0;
+            int idx = idx0;
+            const double* sv = stock + (size_t)v * n + i;
+            for (int k = 0; k < SL; ++k) {
+                dot = fma(__ldg(hrf + idx), sv[(size_t)k * nvoi * n], dot);
+                idx = (idx + 1 == SL) ? 0 : idx + 1;
+            }
+            bold_p[v * n] = (dot - 1.0) * k1v0;
+        }
+        bold_p += (size_t)nvoi * n;
+    }
+
+    // Standard normals of step s from the fed array or the Philox block held in zc.
+    __device__ __forceinline__ void fetch_z(const tvbk_launch& L, int n, int64_t s, float* z) {
+        if constexpr (STOCH) {
+            if (L.noise == TVBK_NOISE_FED) {
+#pragma unroll
+                for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
+                fed_p += (size_t)NINT * n;
+            } else {
+                const int r = (int)(s & 3);
+#pragma unroll
+                for (int k = 0; k < NINT; ++k)
+                    z[k] = (r == 0) ? zc[k][0] : (r == 1) ? zc[k][1] : (r == 2) ? zc[k][2] : zc[k][3];
+            }
+        }
+    }
+
+    // Philox normals of the block of step s into dst (every state variable with a non-zero sigma).
+    __device__ __forceinline__ void philox_block(int i, int64_t s, float (*dst)[4]) {
+        if constexpr (STOCH) {
+#pragma unroll
+            for (int k = 0; k < NINT; ++k)
+                if (NINT == 1 || sig[k] != 0.0f) philox_normals4(seed, stream, s, i, k, dst[k]);
         }
     }
 
@@ -448,36 +582,113 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     const int K = L.sync_every;
     int since_sync = 0;
     int wslot = (int)(s0 % RL);  // slot of the last written time
-    float cnext[NCV];
-    if (PIPE && act) row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
-    for (int ks = 0; ks < nsteps; ++ks) {
-        const int prev = wslot;                     // slot of time s - 1
-        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
-        if (act) {
-            if (STOCH_BLOCK_START(ks)) node.noise_block(L, i, s0 + 1 + ks);
-            float c[NCV];
-            if constexpr (PIPE) {
-#pragma unroll
-                for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
-                // coupling of step s + 1: times s - d with d >= d_min >= 1
-                row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
-            } else {
-                float xi[NCV];
+    // the new state's coupling variables go to the gather ring (and the raw history for SigmoidalJansenRit)
+    auto write = [&](int slot) {
+        if constexpr (SIGMA) {
+            node.write_ring(Ip->ring + (size_t)slot * n * NCV + i * NCV);
+            ring[slot * slot_floats + i] = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+        } else {
+            node.write_ring(ring + slot * slot_floats + i * NCV);
+        }
+    };
+    if constexpr (!PIPE) {
+        for (int ks = 0; ks < nsteps; ++ks) {
+            const int prev = wslot;                     // slot of time s - 1
+            wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
+            if (act) {
+                if (STOCH_BLOCK_START(ks)) node.noise_block(L, i, s0 + 1 + ks);
+                float c[NCV], xi[NCV];
 #pragma unroll
                 for (int k = 0; k < NCV; ++k) xi[k] = node.x[M::cvar(k)];
                 row.couple(ring, prev * slot_floats, ring_floats, xi, cf, c);
+                node.advance(L, Ip, i, n, s0, ks, c);
+                write(wslot);
             }
-            node.advance(L, Ip, i, n, s0, ks, c);
-            if constexpr (SIGMA) {
-                node.write_ring(Ip->ring + (size_t)wslot * n * NCV + i * NCV);  // raw history
-                ring[wslot * slot_floats + i] = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
-            } else {
-                node.write_ring(ring + wslot * slot_floats + i * NCV);
+            if (++since_sync == K) {
+                since_sync = 0;
+                __syncthreads();
             }
         }
-        if (++since_sync == K) {
-            since_sync = 0;
-            __syncthreads();
+    } else {
+        // Blocked loop: steps go in blocks of four aligned to the Philox noise
+        // blocks (s = 4q .. 4q + 3).  A block with no monitor sample before its
+        // last step runs as straight-line code -- the four steps' normals come
+        // from registers, the next block's normals are drawn in between, the
+        // monitors only accumulate, and the samples that fall on its last step
+        // are taken after it; every other step (the launch's first partial
+        // block, blocks with a sample inside, fed noise, a barrier interval
+        // below 4) runs one at a time.  Both paths do the same arithmetic.
+        node.init_clock(Ip, s0);
+        const int nvoi = L.nvoi;
+        const bool fed = L.noise == TVBK_NOISE_FED;
+        int64_t zq = -1;  // Philox block whose normals are in node.zc
+        float cnext[NCV];
+        if (act) row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
+        int64_t s = s0 + 1;  // the step to do next
+        int ks = 0;
+        while (ks < nsteps) {
+            const bool fast = !fed && K >= 4 && (s & 3) == 0 && nsteps - ks >= 4 && node.cd_t >= 4 &&
+                              node.cd_i >= 4 && node.cd_b >= 4;  // uniform over the CTA
+            if (fast) {
+                if (since_sync + 4 > K) {
+                    since_sync = 0;
+                    __syncthreads();
+                }
+                if (act) {
+                    if (SchemeTraits<SCHEME>::stoch && zq != (s >> 2)) node.philox_block(i, s, node.zc);
+                    float zn[M::NINT][4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        float c[NCV], z[M::NINT];
+#pragma unroll
+                        for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
+                        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s + r
+                        row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
+                        if (r == 1) node.philox_block(i, s + 4, zn);  // the next block's normals
+#pragma unroll
+                        for (int k = 0; k < M::NINT; ++k) z[k] = node.zc[k][r];
+                        node.integrate(c, z, L.dt);
+                        node.accumulate(L, n);
+                        write(wslot);
+                    }
+                    if constexpr (SchemeTraits<SCHEME>::stoch) {
+#pragma unroll
+                        for (int k = 0; k < M::NINT; ++k)
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) node.zc[k][r] = zn[k][r];
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
+                }
+                zq = (s >> 2) + 1;
+                node.tick(4, act, s + 3, i, n, nvoi);
+                since_sync += 4;
+                s += 4;
+                ks += 4;
+            } else {
+                wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
+                if (act) {
+                    if (SchemeTraits<SCHEME>::stoch && !fed && zq != (s >> 2)) node.philox_block(i, s, node.zc);
+                    float c[NCV], z[M::NINT];
+#pragma unroll
+                    for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
+                    // coupling of step s + 1: times s - d with d >= d_min >= 1
+                    row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
+                    node.fetch_z(L, n, s, z);
+                    node.integrate(c, z, L.dt);
+                    node.accumulate(L, n);
+                    write(wslot);
+                }
+                zq = s >> 2;
+                node.tick(1, act, s, i, n, nvoi);
+                if (++since_sync == K) {
+                    since_sync = 0;
+                    __syncthreads();
+                }
+                s += 1;
+                ks += 1;
+            }
         }
     }
     __syncthreads();

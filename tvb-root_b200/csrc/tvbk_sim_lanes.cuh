@@ -16,6 +16,7 @@
 #include <cuda_pipeline.h>
 
 #include "tvbk_sim_cluster.cuh"
+#include "tvbk_sim_ws.cuh"
 #include "tvbk_sim_impl.cuh"
 
 namespace tvbk {
@@ -225,6 +226,7 @@ template <class M, int CF, int SCHEME>
 int launch_all_scheme(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
     if (L.lanes > 1) return launch_group<M, CF, SCHEME>(L, st, L.max_degree);
     if (L.cluster > 1) return launch_cluster<M, CF, SCHEME>(L, st);
+    if (L.prefetch == 2) return launch_ws<M, CF, SCHEME>(L, st, smem_bytes);
     return launch_scheme<M, CF, SCHEME>(L, st, smem_bytes, L.max_degree);
 }
 

@@ -9,7 +9,8 @@ different mapping of the work onto the GPU:
 * history tiling: the ring staged in shared memory for the whole launch
   (``ring_in_smem=True``) or read in place from L2 / HBM;
 * the coupling gather: one thread per row with the next step's gather issued
-  ahead (``gather='row'``) or a balanced edge-parallel split (``gather='edge'``).
+  ahead (``gather='row'``), the same with the gather on separate warps
+  (``gather='split'``), or a balanced edge-parallel split (``gather='edge'``).
 
 Which one is fastest depends on the instance count, the region count, the
 horizon, the degree distribution and the model.  ``tune`` runs each variant
@@ -55,11 +56,12 @@ def shape_key(model_id, cfun_id, scheme_id, noise_kind, dt, voi, specs, device):
 def candidates(ncvar, n, n_inst, shared_conn):
     """Variants to try (keyword arguments of ``Batch``)."""
     out = [dict(gather='row', lanes=1, ring_in_smem=None, cluster=0),
+           dict(gather='split', lanes=1, ring_in_smem=True, cluster=0),
            dict(gather='row', lanes=1, ring_in_smem=False, cluster=0),
            dict(gather='edge', lanes=1, ring_in_smem=None, cluster=0)]
     if shared_conn and n_inst % (8 // ncvar) == 0:
         out.append(dict(gather='row', lanes=8 // ncvar, ring_in_smem=None, cluster=0))
-    for C in (2, 4, 8):
+    for C in (2, 4, 8, 16):
         if C <= max(2, -(-n // 32)):
             out.append(dict(gather='row', lanes=1, ring_in_smem=False, cluster=C))
     return out
@@ -100,8 +102,9 @@ def tune(make_batch, key, ncvar, n, n_inst, shared_conn, trial_steps=2000, use_c
             b = make_batch(**cand)
         except (ValueError, _lib.TvbkError):
             continue
-        name = '%s/lanes%d/%s/cluster%d' % (cand['gather'], b.lanes, 'smem' if b.ring_in_smem else 'inplace',
-                                             b.cluster)
+        name = '%s/lanes%d/%s/cluster%d/prefetch%d' % (cand['gather'], b.lanes,
+                                                        'smem' if b.ring_in_smem else 'inplace', b.cluster,
+                                                        b.prefetch)
         if name in timings:
             continue
         try:

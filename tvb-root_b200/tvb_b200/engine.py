@@ -157,13 +157,21 @@ class Batch:
         self.ring_in_smem = bool(ring_in_smem)
         self.edges_per_thread, self.block_threads = 0, 0
         self.prefetch = 0
-        if gather not in ('auto', 'row', 'edge'):
-            raise ValueError("gather must be 'auto', 'row' or 'edge'")
+        if gather not in ('auto', 'row', 'edge', 'split'):
+            raise ValueError("gather must be 'auto', 'row', 'edge' or 'split'")
         if gather != 'edge' and dmin >= 1 and self.cfun_id != _lib.CFUN_IDS['Difference'] \
                 and self.model_id != _lib.MODEL_IDS['Sum']:
             # row kernel with the next step's gather issued ahead: barrier interval K <= d_min
             self.prefetch = 1
             self.sync_every = min(self.sync_every, dmin)
+        if gather == 'split':
+            # separate gather and update warps (the prefetch overlap across warps)
+            ring_b = -(-(hmax + self.sync_every) * self.max_n * self.ncvar_gather * 4 // 16) * 16
+            if not (self.prefetch and self.ring_in_smem and V == 1 and self.max_degree <= 64
+                    and ring_b + 2 * self.max_n * self.ncvar * 4 <= 227 * 1024):
+                raise ValueError('the split gather needs rings in shared memory, delays >= 1, Linear or '
+                                 'SigmoidalJansenRit coupling and row degrees <= 64')
+            self.prefetch = 2
         if gather == 'edge' and V == 1:
             ep = self._choose_edge_parallel(dmin, hmax)
             if ep is not None:
