@@ -59,16 +59,23 @@ enum {
     TVBK_MODEL_SUM = 4         /* dx = x + c; the model of the reference's exact-propagation test */
 };
 enum {
-    TVBK_CFUN_LINEAR = 0,        /* Linear: a*gx + b (coupling.py:170-200) */
+    TVBK_CFUN_LINEAR = 0,        /* Linear: a*gx + b (coupling.py:170-200); Scaling is Linear with b = 0 */
     TVBK_CFUN_DIFFERENCE = 1,    /* Difference: a * sum w (x_j - x_i) (coupling.py:462-486) */
-    TVBK_CFUN_SIGMOIDAL_JR = 2   /* SigmoidalJansenRit (coupling.py:325-376) */
+    TVBK_CFUN_SIGMOIDAL_JR = 2,  /* SigmoidalJansenRit (coupling.py:325-376) */
+    TVBK_CFUN_SIGMOIDAL = 3,     /* Sigmoidal: cmin + (cmax-cmin) / (1 + exp(-a ((gx-midpoint)/sigma))),
+                                  * cfun {cmin, cmax, midpoint, a, sigma} (coupling.py:270-322) */
+    TVBK_CFUN_HYPERBOLIC_TANGENT = 4, /* pre a (1 + tanh((b x_j - midpoint)/sigma)), cfun {a, b, midpoint,
+                                       * sigma} (coupling.py:227-267) */
+    TVBK_CFUN_KURAMOTO = 5       /* pre sin(x_j - x_i), post a / ncvar * gx, cfun {a} (coupling.py:489-508) */
 };
+/* Couplings 3..5 run on the row kernel one step at a time (prefetch 0, lanes 1, no edge split, no cluster). */
 enum {
     TVBK_SCHEME_EULER_DET = 0,   /* integrators.py:365-391 */
     TVBK_SCHEME_EULER_STOCH = 1, /* integrators.py:394-426 */
     TVBK_SCHEME_HEUN_DET = 2,    /* integrators.py:286-318 */
     TVBK_SCHEME_HEUN_STOCH = 3,  /* integrators.py:321-362 */
-    TVBK_SCHEME_IDENTITY = 4     /* integrators.py:483-507 */
+    TVBK_SCHEME_IDENTITY = 4,    /* integrators.py:483-507 */
+    TVBK_SCHEME_RK4 = 5          /* RungeKutta4thOrderDeterministic, integrators.py:429-480 */
 };
 enum {
     TVBK_NOISE_NONE = 0,

@@ -180,18 +180,27 @@ def coupling_sparse(kind, buf, step, lay, params):
     x_j = buf[t_idx[None, :], np.arange(buf.shape[1])[:, None], lay['col'][None, :]]
     current = buf[(step - 1) % H]
     x_i = current[:, lay['row']]
-    if kind in ('Linear', 'PassThrough'):
+    if kind in ('Linear', 'PassThrough', 'Scaling', 'Sigmoidal'):
         pre = x_j
     elif kind == 'Difference':
         pre = x_j - x_i
+    elif kind == 'HyperbolicTangent':                          # coupling.py:259-260
+        pre = params['a'] * (1 + np.tanh((params['b'] * x_j - params['midpoint']) / params['sigma']))
+    elif kind == 'Kuramoto':                                   # coupling.py:504-505
+        pre = np.sin(x_j - x_i)
     else:
         raise NotImplementedError(kind)
-    out = np.zeros_like(current)
+    out = np.zeros(current.shape, dtype=pre.dtype)
     out[:, lay['nzr']] = np.add.reduceat(lay['w'][None, :] * pre, lay['lri'], axis=1)
     if kind == 'Linear':
         return params['a'] * out + params['b']
-    if kind == 'Difference':
+    if kind in ('Difference', 'Scaling'):                      # coupling.py:220-221,485-486
         return params['a'] * out
+    if kind == 'Sigmoidal':                                    # coupling.py:316-317
+        return params['cmin'] + ((params['cmax'] - params['cmin']) /
+                                 (1.0 + np.exp(-params['a'] * ((out - params['midpoint']) / params['sigma']))))
+    if kind == 'Kuramoto':                                     # coupling.py:507-508 (a / gx.shape[0])
+        return params['a'] / out.shape[0] * out
     return out
 
 
@@ -368,6 +377,16 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
     elif coupling == 'SigmoidalJansenRit':
         for k, v in dict(cmin=0.0, cmax=2.0 * 0.0025, midpoint=6.0, r=0.56, a=1.0).items():
             cp.setdefault(k, np.array(v))
+    elif coupling == 'Scaling':
+        cp.setdefault('a', np.array(0.00390625))
+    elif coupling == 'HyperbolicTangent':
+        for k, v in dict(a=1.0, b=1.0, midpoint=0.0, sigma=1.0).items():
+            cp.setdefault(k, np.array(v))
+    elif coupling == 'Sigmoidal':
+        for k, v in dict(cmin=-1.0, cmax=1.0, midpoint=0.0, a=1.0, sigma=230.0).items():
+            cp.setdefault(k, np.array(v))
+    elif coupling == 'Kuramoto':
+        cp.setdefault('a', np.array(1.0))
 
     def couple(step):
         if coupling == 'SigmoidalJansenRit':
@@ -432,6 +451,19 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
             X = X + dX + gfun * noise + dt * 0.0
         elif integrator == 'Identity':                 # integrators.py:494-507
             X = dfun(X, c, p) + 0.0
+        elif integrator == 'RungeKutta4thOrderDeterministic':   # integrators.py:437-480
+            dt2, dt6 = dt / 2.0, dt / 6.0
+            k1 = dfun(X, c, p)
+            i1 = X + dt2 * k1
+            bound(i1)
+            k2 = dfun(i1, c, p)
+            i2 = X + dt2 * k2
+            bound(i2)
+            k3 = dfun(i2, c, p)
+            i3 = X + dt * k3
+            bound(i3)
+            k4 = dfun(i3, c, p)
+            X = X + dt6 * (k1 + 2.0 * k2 + 2.0 * k3 + k4) + dt * 0.0
         else:
             raise NotImplementedError(integrator)
         bound(X)

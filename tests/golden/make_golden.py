@@ -450,6 +450,53 @@ def case_difference(R):
          a=0.1, linear=res_lin[:, :, 0], linear_a=0.5, linear_b=0.25)
 
 
+def case_couplings(R):
+    """The couplings beyond Linear / Difference / SigmoidalJansenRit and the
+    Runge-Kutta scheme: Generic2dOscillator, 40 regions (40 % density, tract
+    lengths 10-120 mm, speed 3 mm/ms), Raw, 40 ms at dt 0.1 with Scaling,
+    Sigmoidal, HyperbolicTangent, Kuramoto (HeunDeterministic) and Linear with
+    RungeKutta4thOrderDeterministic; Epileptor (two coupling variables) with
+    HyperbolicTangent, HeunDeterministic dt 0.05, TemporalAverage 1 ms, 20 ms."""
+    w, L = synthetic_connectome(40, 0.40, 10.0, 120.0, seed=21)
+    speed = 3.0
+    C, I = R['coupling'], R['integrators']
+    cases = {
+        'scaling': (C.Scaling(a=np.array([0.02])), I.HeunDeterministic(dt=0.1)),
+        'sigmoidal': (C.Sigmoidal(cmin=np.array([-0.5]), cmax=np.array([0.5]), midpoint=np.array([0.5]),
+                                  a=np.array([1.2]), sigma=np.array([4.0])), I.HeunDeterministic(dt=0.1)),
+        'tanh': (C.HyperbolicTangent(a=np.array([0.05]), b=np.array([0.8]), midpoint=np.array([0.3]),
+                                     sigma=np.array([2.0])), I.HeunDeterministic(dt=0.1)),
+        'kuramoto': (C.Kuramoto(a=np.array([0.3])), I.HeunDeterministic(dt=0.1)),
+        'rk4': (C.Linear(a=np.array([0.0152])), I.RungeKutta4thOrderDeterministic(dt=0.1)),
+    }
+    out = dict(weights=w, tract_lengths=L, speed=speed, conn_recipe=np.array([40, 0.40, 10.0, 120.0, 21]),
+               ic_seed=202)
+    for name, (cf, integ) in cases.items():
+        def build(cf=cf, integ=integ):
+            return R['simulator'].Simulator(
+                model=R['models'].Generic2dOscillator(), connectivity=make_conn(R, w, L, speed), coupling=cf,
+                integrator=integ, monitors=[R['monitors'].Raw()], simulation_length=40.0)
+        sim, cfg, res, _, _ = run_sim(R, build, 40.0, False, ic_seed=202)
+        (t, raw), = res
+        out[name + '_raw'] = raw[..., 0]
+        out[name + '_t'] = t
+        out[name + '_buffer0'] = cfg['buffer0']
+        out[name + '_state0'] = cfg['state0']
+
+    def build_epi():
+        return R['simulator'].Simulator(
+            model=R['models'].Epileptor(), connectivity=make_conn(R, w, L, speed),
+            coupling=C.HyperbolicTangent(a=np.array([0.02]), b=np.array([1.0]), midpoint=np.array([-1.0]),
+                                         sigma=np.array([1.5])),
+            integrator=I.HeunDeterministic(dt=0.05), monitors=[R['monitors'].TemporalAverage(period=1.0)],
+            simulation_length=20.0)
+    sim, cfg, res, _, _ = run_sim(R, build_epi, 20.0, False, ic_seed=203)
+    (t, tavg), = res
+    out.update(epi_tanh_tavg=tavg[..., 0], epi_tanh_t=t, epi_tanh_buffer0=cfg['buffer0'],
+               epi_tanh_state0=cfg['state0'])
+    save('couplings_40', **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference/tvb_library')
@@ -476,6 +523,7 @@ def main():
                                       10000.0, True),
         'rww_full': lambda: case_rww(R, 'rww_68_full', [(16, 16), (31, 8)], 60000.0, False),
         'jr': lambda: case_jr(R),
+        'couplings': lambda: case_couplings(R),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only:

@@ -374,3 +374,44 @@ def test_chunked_graph_replay_matches_one_launch():
             assert sw.batch._graph_launches >= 2
     np.testing.assert_array_equal(outs['eager'], outs['one'])
     np.testing.assert_array_equal(outs['graph'], outs['one'])
+
+
+@pytest.mark.parametrize('case', ['scaling', 'sigmoidal', 'tanh', 'kuramoto', 'rk4'])
+def test_more_couplings_and_rk4_vs_reference(case):
+    """Scaling, Sigmoidal, HyperbolicTangent, Kuramoto (coupling.py:203-322,489-508) and
+    RungeKutta4thOrderDeterministic (integrators.py:429-480) on Generic2dOscillator, 40 regions,
+    40 ms, against the reference's own runs."""
+    T = tvb()
+    fx = G.load('couplings_40')
+    cf = {'scaling': lambda c: c.Scaling(a=0.02),
+          'sigmoidal': lambda c: c.Sigmoidal(cmin=-0.5, cmax=0.5, midpoint=0.5, a=1.2, sigma=4.0),
+          'tanh': lambda c: c.HyperbolicTangent(a=0.05, b=0.8, midpoint=0.3, sigma=2.0),
+          'kuramoto': lambda c: c.Kuramoto(a=0.3),
+          'rk4': lambda c: c.Linear(a=0.0152)}[case](T['coupling'])
+    integ = (T['integrators'].RungeKutta4thOrderDeterministic(dt=0.1) if case == 'rk4'
+             else T['integrators'].HeunDeterministic(dt=0.1))
+    np.random.seed(int(fx['ic_seed']))
+    sim = T['Simulator'](model=T['models'].Generic2dOscillator(),
+                         connectivity=T['Connectivity'](weights=fx['weights'], tract_lengths=fx['tract_lengths'],
+                                                        speed=float(fx['speed'])),
+                         coupling=cf, integrator=integ, monitors=[T['monitors'].Raw()],
+                         simulation_length=40.0).configure()
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx[case + '_buffer0'])
+    (t, raw), = sim.run()
+    np.testing.assert_allclose(t, fx[case + '_t'], rtol=0, atol=1e-12)
+    report('%s raw vs reference' % case, raw[..., 0], fx[case + '_raw'], 1e-4)
+
+
+def test_epileptor_hyperbolic_tangent_vs_reference():
+    T = tvb()
+    fx = G.load('couplings_40')
+    np.random.seed(203)
+    sim = T['Simulator'](model=T['models'].Epileptor(),
+                         connectivity=T['Connectivity'](weights=fx['weights'], tract_lengths=fx['tract_lengths'],
+                                                        speed=float(fx['speed'])),
+                         coupling=T['coupling'].HyperbolicTangent(a=0.02, b=1.0, midpoint=-1.0, sigma=1.5),
+                         integrator=T['integrators'].HeunDeterministic(dt=0.05),
+                         monitors=[T['monitors'].TemporalAverage(period=1.0)], simulation_length=20.0).configure()
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx['epi_tanh_buffer0'])
+    (t, tavg), = sim.run()
+    report('epileptor tanh tavg vs reference', tavg[..., 0], fx['epi_tanh_tavg'], 1e-4)

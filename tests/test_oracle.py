@@ -189,3 +189,33 @@ def test_jansen_rit_sigmoidal_heun_stochastic_prefix():
     idx = fx['tavg_index']
     k = int(np.sum(idx < 200))
     np.testing.assert_allclose(out[0][1][idx[:k]], fx['tavg'][:k], rtol=1e-9, atol=1e-11)
+
+
+@pytest.mark.parametrize('case,coupling,params,integrator', [
+    ('scaling', 'Scaling', {'a': 0.02}, 'HeunDeterministic'),
+    ('sigmoidal', 'Sigmoidal', {'cmin': -0.5, 'cmax': 0.5, 'midpoint': 0.5, 'a': 1.2, 'sigma': 4.0},
+     'HeunDeterministic'),
+    ('tanh', 'HyperbolicTangent', {'a': 0.05, 'b': 0.8, 'midpoint': 0.3, 'sigma': 2.0}, 'HeunDeterministic'),
+    ('kuramoto', 'Kuramoto', {'a': 0.3}, 'HeunDeterministic'),
+    ('rk4', 'Linear', {'a': 0.0152}, 'RungeKutta4thOrderDeterministic')])
+def test_more_couplings_and_rk4(case, coupling, params, integrator):
+    """Scaling, Sigmoidal, HyperbolicTangent, Kuramoto (coupling.py:203-322,489-508) and
+    RungeKutta4thOrderDeterministic (integrators.py:429-480) against reference runs."""
+    fx = G.load('couplings_40')
+    w, L = fx['weights'], fx['tract_lengths']
+    out, _ = O.simulate('Generic2dOscillator', {}, w, L, float(fx['speed']), 0.1, coupling, params, integrator,
+                        400, [O.Monitor('Raw')], fx[case + '_buffer0'], fx[case + '_state0'], 0)
+    ref = fx[case + '_raw']
+    err = np.abs(out[0][1] - ref).max() / np.abs(ref).max()
+    assert err < 1e-9, (case, err)
+
+
+def test_epileptor_hyperbolic_tangent_two_cvars():
+    fx = G.load('couplings_40')
+    out, _ = O.simulate('Epileptor', {}, fx['weights'], fx['tract_lengths'], float(fx['speed']), 0.05,
+                        'HyperbolicTangent', {'a': 0.02, 'b': 1.0, 'midpoint': -1.0, 'sigma': 1.5},
+                        'HeunDeterministic', 400, [O.Monitor('TemporalAverage', 1.0)],
+                        fx['epi_tanh_buffer0'], fx['epi_tanh_state0'], 0)
+    ref = fx['epi_tanh_tavg']
+    err = np.abs(out[0][1] - ref).max() / np.abs(ref).max()
+    assert err < 1e-9, err

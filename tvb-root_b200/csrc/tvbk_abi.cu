@@ -206,6 +206,12 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
     if (stoch && L->noise != TVBK_NOISE_FED && L->noise != TVBK_NOISE_PHILOX)
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: stochastic scheme needs fed or Philox noise");
     if (L->max_steps == 0) return TVBK_OK;
+    if (L->cfun < 0 || L->cfun > TVBK_CFUN_KURAMOTO)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: unknown coupling %d", L->cfun);
+    if (L->cfun >= TVBK_CFUN_SIGMOIDAL && (L->prefetch != 0 || L->lanes > 1 || L->edges_per_thread != 0 ||
+                                           L->cluster > 1))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: Sigmoidal, HyperbolicTangent and Kuramoto run on the row kernel "
+                    "one step at a time (prefetch 0, lanes 1, edges_per_thread 0, cluster 0)");
     if (L->cluster < 0 || L->cluster > 16)
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster %d out of 0..16", L->cluster);
     if (L->cluster > 1) {

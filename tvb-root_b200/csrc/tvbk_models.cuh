@@ -186,7 +186,9 @@ struct SumModel {
 // Coupling kinds: the gather accumulates sum_j w_ij * pre(x_i, x_j(t - d_ij)),
 // post() maps the sums to the model's coupling input.
 
-enum { CF_LINEAR = 0, CF_DIFFERENCE = 1, CF_SIGMOIDAL_JR = 2 };
+enum { CF_LINEAR = 0, CF_DIFFERENCE = 1, CF_SIGMOIDAL_JR = 2, CF_GENERIC = 3 };
+// CF_GENERIC kernels serve TVBK_CFUN_SIGMOIDAL, _HYPERBOLIC_TANGENT and _KURAMOTO, choosing
+// the pre / post forms at run time from the launch's coupling code.
 
 template <int CF>
 struct CouplingTraits;

@@ -8,6 +8,9 @@ int launch_epileptor_euler_stoch(const tvbk_launch& L, cudaStream_t st, size_t s
         case CF_LINEAR: return launch_all_scheme<Epileptor, CF_LINEAR, TVBK_SCHEME_EULER_STOCH>(L, st, smem_bytes);
         case CF_DIFFERENCE: return launch_all_scheme<Epileptor, CF_DIFFERENCE, TVBK_SCHEME_EULER_STOCH>(L, st, smem_bytes);
         case CF_SIGMOIDAL_JR: return launch_all_scheme<Epileptor, CF_SIGMOIDAL_JR, TVBK_SCHEME_EULER_STOCH>(L, st, smem_bytes);
+        case TVBK_CFUN_SIGMOIDAL:
+        case TVBK_CFUN_HYPERBOLIC_TANGENT:
+        case TVBK_CFUN_KURAMOTO: return launch_all_scheme<Epileptor, CF_GENERIC, TVBK_SCHEME_EULER_STOCH>(L, st, smem_bytes);
         default: return -2;
     }
 }

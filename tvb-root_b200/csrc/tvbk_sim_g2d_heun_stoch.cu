@@ -7,6 +7,9 @@ int launch_g2d_heun_stoch(const tvbk_launch& L, cudaStream_t st, size_t smem_byt
     switch (L.cfun) {
         case CF_LINEAR: return launch_all_scheme<G2D, CF_LINEAR, TVBK_SCHEME_HEUN_STOCH>(L, st, smem_bytes);
         case CF_DIFFERENCE: return launch_all_scheme<G2D, CF_DIFFERENCE, TVBK_SCHEME_HEUN_STOCH>(L, st, smem_bytes);
+        case TVBK_CFUN_SIGMOIDAL:
+        case TVBK_CFUN_HYPERBOLIC_TANGENT:
+        case TVBK_CFUN_KURAMOTO: return launch_all_scheme<G2D, CF_GENERIC, TVBK_SCHEME_HEUN_STOCH>(L, st, smem_bytes);
         default: return -2;
     }
 }

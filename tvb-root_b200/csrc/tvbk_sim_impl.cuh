@@ -39,10 +39,31 @@ struct SchemeTraits {
 // where a new block of four Philox normals starts.
 #define STOCH_BLOCK_START(ks) ((ks) == 0 || ((s0 + 1 + (ks)) & 3) == 0)
 
+// Per-edge pre() forms of the couplings whose pre / post are chosen at run
+// time (CF_GENERIC kernels): HyperbolicTangent a (1 + tanh((b x_j - midpoint)
+// / sigma)) (coupling.py:263-264) and Kuramoto sin(x_j - x_i)
+// (coupling.py:504-505); Sigmoidal gathers x_j like Linear.
+enum { PRE_TANH = 100, PRE_SIN = 101 };
+
 // acc += w * pre(x_i, x_j) for one edge whose delayed value(s) start at src.
 template <int CF, int NCV>
 __device__ __forceinline__ void accumulate(float* acc, float w, const float* src, const float* xi, const float* cf) {
-    if constexpr (NCV == 1) {
+    if constexpr (CF == PRE_TANH || CF == PRE_SIN) {
+        float v[NCV];
+        if constexpr (NCV == 1) {
+            v[0] = src[0];
+        } else {
+            const float2 t = *reinterpret_cast<const float2*>(src);
+            v[0] = t.x;
+            v[1] = t.y;
+        }
+#pragma unroll
+        for (int k = 0; k < NCV; ++k) {
+            const float pre = (CF == PRE_TANH) ? cf[0] * (1.0f + tanhf((cf[1] * v[k] - cf[2]) / cf[3]))
+                                               : sinf(v[k] - xi[k]);
+            acc[k] = fmaf(w, pre, acc[k]);
+        }
+    } else if constexpr (NCV == 1) {
         const float v = src[0];
         if constexpr (CF == CF_DIFFERENCE)
             acc[0] = fmaf(w, v - xi[0], acc[0]);
@@ -76,6 +97,23 @@ __device__ __forceinline__ void post(const float* acc, const float* cf, float* c
         c[0] = cf[4] * acc[0];
 #pragma unroll
         for (int k = 1; k < NCV; ++k) c[k] = 0.0f;
+    }
+}
+
+// post() of the run-time chosen couplings: Sigmoidal cmin + (cmax - cmin) /
+// (1 + exp(-a ((gx - midpoint) / sigma))) with cf = {cmin, cmax, midpoint, a,
+// sigma} (coupling.py:321-322); HyperbolicTangent gx; Kuramoto a / ncvar * gx
+// (coupling.py:507-508, which divides by gx.shape[0], the coupling variables).
+template <int NCV>
+__device__ __forceinline__ void post_generic(const float* acc, const float* cf, int kind, float* c) {
+#pragma unroll
+    for (int k = 0; k < NCV; ++k) {
+        if (kind == TVBK_CFUN_SIGMOIDAL)
+            c[k] = cf[0] + (cf[1] - cf[0]) / (1.0f + expf(-cf[3] * ((acc[k] - cf[2]) / cf[4])));
+        else if (kind == TVBK_CFUN_KURAMOTO)
+            c[k] = cf[0] / (float)NCV * acc[k];
+        else
+            c[k] = acc[k];
     }
 }
 
@@ -131,11 +169,11 @@ struct RegRow {
         }
     }
 
-    __device__ __forceinline__ void couple(const float* __restrict__ ring, int base_off, int ring_floats,
-                                           const float* xi, const float* cf, float* c) const {
-        constexpr int NCV = M::NCV;
-        constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
-        float a0[NG], a1[NG];
+    // a0 = sum over the row of w * pre (two partial sums: even / odd slots)
+    template <int GCF, int NG>
+    __device__ __forceinline__ void sum(const float* __restrict__ ring, int base_off, int ring_floats,
+                                        const float* xi, const float* cf, float* a0) const {
+        float a1[NG];
 #pragma unroll
         for (int k = 0; k < NG; ++k) a0[k] = a1[k] = 0.0f;
         const char* rb = reinterpret_cast<const char*>(ring);
@@ -147,7 +185,27 @@ struct RegRow {
         }
 #pragma unroll
         for (int k = 0; k < NG; ++k) a0[k] += a1[k];
-        post<CF, NCV>(a0, cf, c);
+    }
+
+    // kind: the launch's coupling code, read by the run-time chosen couplings (CF_GENERIC)
+    __device__ __forceinline__ void couple(const float* __restrict__ ring, int base_off, int ring_floats,
+                                           const float* xi, const float* cf, float* c, int kind = 0) const {
+        constexpr int NCV = M::NCV;
+        if constexpr (CF == CF_GENERIC) {
+            float a[NCV];
+            if (kind == TVBK_CFUN_HYPERBOLIC_TANGENT)
+                sum<PRE_TANH, NCV>(ring, base_off, ring_floats, xi, cf, a);
+            else if (kind == TVBK_CFUN_KURAMOTO)
+                sum<PRE_SIN, NCV>(ring, base_off, ring_floats, xi, cf, a);
+            else
+                sum<CF_LINEAR, NCV>(ring, base_off, ring_floats, xi, cf, a);
+            post_generic<NCV>(a, cf, kind, c);
+        } else {
+            constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
+            float a[NG];
+            sum<GCF, NG>(ring, base_off, ring_floats, xi, cf, a);
+            post<CF, NCV>(a, cf, c);
+        }
     }
 };
 
@@ -162,11 +220,10 @@ struct RegRow<M, CF, 0> {
         deg = e1 - e0;
     }
 
-    __device__ __forceinline__ void couple(const float* __restrict__ ring, int base_off, int ring_floats,
-                                           const float* xi, const float* cf, float* c) const {
-        constexpr int NCV = M::NCV;
-        constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
-        float a0[NG], a1[NG];
+    template <int GCF, int NG>
+    __device__ __forceinline__ void sum(const float* __restrict__ ring, int base_off, int ring_floats,
+                                        const float* xi, const float* cf, float* a0) const {
+        float a1[NG];
 #pragma unroll
         for (int k = 0; k < NG; ++k) a0[k] = a1[k] = 0.0f;
         int e = 0;
@@ -181,7 +238,26 @@ struct RegRow<M, CF, 0> {
         }
 #pragma unroll
         for (int k = 0; k < NG; ++k) a0[k] += a1[k];
-        post<CF, NCV>(a0, cf, c);
+    }
+
+    __device__ __forceinline__ void couple(const float* __restrict__ ring, int base_off, int ring_floats,
+                                           const float* xi, const float* cf, float* c, int kind = 0) const {
+        constexpr int NCV = M::NCV;
+        if constexpr (CF == CF_GENERIC) {
+            float a[NCV];
+            if (kind == TVBK_CFUN_HYPERBOLIC_TANGENT)
+                sum<PRE_TANH, NCV>(ring, base_off, ring_floats, xi, cf, a);
+            else if (kind == TVBK_CFUN_KURAMOTO)
+                sum<PRE_SIN, NCV>(ring, base_off, ring_floats, xi, cf, a);
+            else
+                sum<CF_LINEAR, NCV>(ring, base_off, ring_floats, xi, cf, a);
+            post_generic<NCV>(a, cf, kind, c);
+        } else {
+            constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
+            float a[NG];
+            sum<GCF, NG>(ring, base_off, ring_floats, xi, cf, a);
+            post<CF, NCV>(a, cf, c);
+        }
     }
 };
 
@@ -282,6 +358,23 @@ struct Node {
             const float hdt = dt * 0.5f;
 #pragma unroll
             for (int k = 0; k < NSV; ++k) x[k] = x[k] + (m0[k] + m1[k]) * hdt + nz[k];
+        } else if constexpr (SCHEME == TVBK_SCHEME_RK4) {
+            const float dt2 = dt * 0.5f, dt6 = dt / 6.0f;
+            float st[NSV], k2[NSV], k3[NSV], k4[NSV];
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) st[k] = x[k] + dt2 * m0[k];
+            M::bound(st);
+            M::dfun(st, c, p, k2);
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) st[k] = x[k] + dt2 * k2[k];
+            M::bound(st);
+            M::dfun(st, c, p, k3);
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) st[k] = x[k] + dt * k3[k];
+            M::bound(st);
+            M::dfun(st, c, p, k4);
+#pragma unroll
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt6 * (m0[k] + 2.0f * k2[k] + 2.0f * k3[k] + k4[k]);
         } else {  // identity
 #pragma unroll
             for (int k = 0; k < NSV; ++k) x[k] = m0[k];
@@ -600,7 +693,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                 float c[NCV], xi[NCV];
 #pragma unroll
                 for (int k = 0; k < NCV; ++k) xi[k] = node.x[M::cvar(k)];
-                row.couple(ring, prev * slot_floats, ring_floats, xi, cf, c);
+                row.couple(ring, prev * slot_floats, ring_floats, xi, cf, c, L.cfun);
                 node.advance(L, Ip, i, n, s0, ks, c);
                 write(wslot);
             }
@@ -857,7 +950,7 @@ int launch_one(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
 template <class M, int CF, int SCHEME, bool SMEM, int MAXT>
 int launch_deg(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes, int max_deg) {
     if (max_deg <= 0) return launch_one<M, CF, SCHEME, SMEM, MAXT, 0>(L, st, smem_bytes);
-    if constexpr (CF != CF_DIFFERENCE) {
+    if constexpr (CF != CF_DIFFERENCE && CF != CF_GENERIC) {
         if (L.prefetch) {
             if (max_deg <= 32) return launch_one<M, CF, SCHEME, SMEM, MAXT, 32, true>(L, st, smem_bytes);
             if (max_deg <= 64) return launch_one<M, CF, SCHEME, SMEM, MAXT, 64, true>(L, st, smem_bytes);
@@ -882,7 +975,7 @@ int launch_ep(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
 template <class M, int CF, int SCHEME>
 int launch_scheme(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes, int max_deg) {
     if (L.edges_per_thread > 0) {
-        if constexpr (CF == CF_DIFFERENCE) {
+        if constexpr (CF == CF_DIFFERENCE || CF == CF_GENERIC) {
             return -2;
         } else {
             if (!L.ring_in_smem) return -2;

@@ -224,9 +224,14 @@ int launch_group(const tvbk_launch& L, cudaStream_t st, int max_deg) {
 // of CTAs per instance, else the row / edge-parallel kernels.
 template <class M, int CF, int SCHEME>
 int launch_all_scheme(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
-    if (L.lanes > 1) return launch_group<M, CF, SCHEME>(L, st, L.max_degree);
-    if (L.cluster > 1) return launch_cluster<M, CF, SCHEME>(L, st);
-    if (L.prefetch == 2) return launch_ws<M, CF, SCHEME>(L, st, smem_bytes);
+    if constexpr (CF == CF_GENERIC) {
+        // run-time chosen couplings: the row kernel, one step at a time
+        if (L.lanes > 1 || L.cluster > 1 || L.prefetch != 0) return -2;
+    } else {
+        if (L.lanes > 1) return launch_group<M, CF, SCHEME>(L, st, L.max_degree);
+        if (L.cluster > 1) return launch_cluster<M, CF, SCHEME>(L, st);
+        if (L.prefetch == 2) return launch_ws<M, CF, SCHEME>(L, st, smem_bytes);
+    }
     return launch_scheme<M, CF, SCHEME>(L, st, smem_bytes, L.max_degree);
 }
 

@@ -21,9 +21,12 @@ TVBK_STATUS_NONFINITE = 1
 TVBK_STATUS_DEGREE = 2
 
 MODEL_IDS = {'Generic2dOscillator': 0, 'JansenRit': 1, 'ReducedWongWang': 2, 'Epileptor': 3, 'Sum': 4}
-CFUN_IDS = {'Linear': 0, 'Difference': 1, 'SigmoidalJansenRit': 2}
+CFUN_IDS = {'Linear': 0, 'Difference': 1, 'SigmoidalJansenRit': 2, 'Sigmoidal': 3, 'HyperbolicTangent': 4,
+            'Kuramoto': 5}
+# couplings whose kernel runs the row gather one step at a time with the pre / post chosen at run time
+CFUN_GENERIC = (3, 4, 5)
 SCHEME_IDS = {'EulerDeterministic': 0, 'EulerStochastic': 1, 'HeunDeterministic': 2,
-              'HeunStochastic': 3, 'Identity': 4}
+              'HeunStochastic': 3, 'Identity': 4, 'RungeKutta4thOrderDeterministic': 5}
 NOISE_NONE, NOISE_FED, NOISE_PHILOX = 0, 1, 2
 MAX_REGIONS = 1024
 MAX_VOI = 8

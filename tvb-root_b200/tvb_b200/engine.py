@@ -159,8 +159,12 @@ class Batch:
         self.prefetch = 0
         if gather not in ('auto', 'row', 'edge', 'split'):
             raise ValueError("gather must be 'auto', 'row', 'edge' or 'split'")
+        self.generic = self.cfun_id in _lib.CFUN_GENERIC
+        if self.generic and (gather in ('edge', 'split') or V != 1):
+            raise ValueError('Sigmoidal, HyperbolicTangent and Kuramoto run on the row gather, one instance '
+                             'per CTA')
         if gather != 'edge' and dmin >= 1 and self.cfun_id != _lib.CFUN_IDS['Difference'] \
-                and self.model_id != _lib.MODEL_IDS['Sum']:
+                and self.model_id != _lib.MODEL_IDS['Sum'] and not self.generic:
             # row kernel with the next step's gather issued ahead: barrier interval K <= d_min
             self.prefetch = 1
             self.sync_every = min(self.sync_every, dmin)
@@ -211,6 +215,7 @@ class Batch:
         threads = -(-self.max_n * G // 32) * 32
         smem = -(-self.max_n * self.max_degree * 8 // 16) * 16 + 2 * self.max_degree * self.ncvar * threads * 4
         ok = (same and gather != 'edge' and self.model_id != _lib.MODEL_IDS['Sum'] and threads <= 1024
+              and self.cfun_id not in _lib.CFUN_GENERIC
               and smem <= 227 * 1024 and len(specs) % G == 0)
         if ok:
             return G
@@ -231,7 +236,7 @@ class Batch:
         if cluster in (None, 0, 1, '0', '1'):
             return 0, 0
         able = (self.lanes == 1 and not self.ring_in_smem and not self.edges_per_thread
-                and self.model_id != _lib.MODEL_IDS['Sum'])
+                and self.model_id != _lib.MODEL_IDS['Sum'] and not self.generic)
         if cluster == 'auto':
             if not able or self.max_n < 64:
                 return 0, 0

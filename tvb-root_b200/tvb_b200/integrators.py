@@ -47,5 +47,10 @@ class Identity(Integrator):
     """integrators.py:483-507: x_{n+1} = f(x_n)."""
 
 
+class RungeKutta4thOrderDeterministic(Integrator):
+    """integrators.py:429-480: the classical four-stage Runge-Kutta step, the
+    coupling held fixed over the step, bounds applied to each stage."""
+
+
 INTEGRATORS = {cls.__name__: cls for cls in (HeunDeterministic, HeunStochastic, EulerDeterministic,
-                                             EulerStochastic, Identity)}
+                                             EulerStochastic, Identity, RungeKutta4thOrderDeterministic)}

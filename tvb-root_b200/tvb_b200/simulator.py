@@ -163,7 +163,7 @@ class Simulator:
         self.monitors = [adopt_monitor(m) for m in self.monitors]
         name = type(self.model).__name__
         self._model_id = _lib.MODEL_IDS[name]
-        cname = type(self.coupling).__name__
+        cname = getattr(type(self.coupling), 'kernel_id', type(self.coupling).__name__)
         if cname not in _lib.CFUN_IDS:
             raise NotImplementedError('coupling %s' % cname)
         self._cfun_id = _lib.CFUN_IDS[cname]
@@ -329,6 +329,102 @@ class Simulator:
                 if any(r is not None for r in row):
                     yield row
             left -= k
+
+    # ------------------------------------------------------ checkpoint / resume
+    def history_state(self):
+        """The simulation's state in the layout of the framework's
+        SimulationHistory (tvb_framework/tvb/core/entities/file/simulator/
+        simulation_history_h5.py:32-118), as a dict:
+
+        history (H, ncvar, n, 1) float32 and current_state (nsv, n, 1) as the
+        reference's history.buffer and current_state; current_step;
+        monitor_stock_<k> for the k-th monitor (1-based): Raw an empty array,
+        TemporalAverage (istep, nvoi_k, n, 1) holding the current period's sum
+        in row 0 (the reference's stock rows are only ever read as their mean
+        at the next sample, which this reproduces), Bold the 4 ms stock
+        (stock_len, nvoi_k, n, 1) float64; monitor_names; for stochastic
+        schemes the noise RandomState as integrator_noise_rng_state_*.  Also
+        monitor_interim_<k>, Bold's running 4 ms sum (nvoi_k, n, 1), which the
+        reference does not store (it restarts that average on reload).
+        """
+        if not self._configured:
+            raise RuntimeError('call configure() first')
+        n = self.number_of_nodes
+        st = {'history': self.history_buffer.copy(), 'current_state': np.array(self.current_state, copy=True),
+              'current_step': int(self.current_step), 'monitor_names': []}
+        acc = self._acc or {}
+        for k, m in enumerate(self.monitors):
+            name = 'monitor_stock_%d' % (k + 1)
+            st['monitor_names'].append(type(m).__name__)
+            voi = np.asarray(m.voi, dtype=int)
+            if isinstance(m, monitors_mod.TemporalAverage):
+                stock = np.zeros((m.istep, voi.size, n, 1))
+                if 'tavg_acc' in acc:
+                    stock[0, :, :, 0] = acc['tavg_acc'][voi]
+                st[name] = stock
+            elif isinstance(m, monitors_mod.Bold):
+                SL = m.hemodynamic_response_function.shape[1]
+                stock = np.zeros((SL, voi.size, n, 1))
+                interim = np.zeros((voi.size, n, 1))
+                if 'bold_stock' in acc:
+                    stock[..., 0] = acc['bold_stock'][:, voi]
+                    interim[..., 0] = acc['bold_acc'][voi]
+                st[name] = stock
+                st['monitor_interim_%d' % (k + 1)] = interim
+            else:
+                st[name] = np.empty([])
+        if self.integrator.stochastic:
+            algo, keys, pos, has_gauss, cached = self.integrator.noise.random_stream.get_state()
+            st.update(integrator_noise_rng_state_algo=algo, integrator_noise_rng_state_keys=keys,
+                      integrator_noise_rng_state_pos=pos, integrator_noise_rng_state_has_gauss=has_gauss,
+                      integrator_noise_rng_state_cached_gauss=cached)
+        return st
+
+    def set_history_state(self, st):
+        """Resume from a dict produced by ``history_state`` (or a reference
+        SimulationHistory's fields): the next run continues from that step."""
+        if not self._configured:
+            raise RuntimeError('call configure() first')
+        n = self.number_of_nodes
+        hist = np.asarray(st['history'], dtype=np.float32)
+        if hist.ndim == 3:
+            hist = hist[..., None]
+        if hist.shape != self.history_buffer.shape:
+            raise ValueError('history shape %s, expected %s' % (hist.shape, self.history_buffer.shape))
+        self.history_buffer = hist.copy()
+        cs = np.asarray(st['current_state'], dtype=np.float64)
+        self.current_state = (cs if cs.ndim == 3 else cs[..., None]).copy()
+        self.current_step = int(st['current_step'])
+        nvoi = len(self._voi_codes)
+        acc = {}
+        names = list(st.get('monitor_names', [type(m).__name__ for m in self.monitors]))
+        for k, m in enumerate(self.monitors):
+            if k < len(names) and names[k] != type(m).__name__:
+                raise ValueError('monitor %d is %s in the stored state, %s here' % (k + 1, names[k], type(m).__name__))
+            stock = st.get('monitor_stock_%d' % (k + 1))
+            voi = np.asarray(m.voi, dtype=int)
+            if isinstance(m, monitors_mod.TemporalAverage) and stock is not None:
+                t = np.zeros((nvoi, n), dtype=np.float32)
+                ph = self.current_step % m.istep
+                t[voi] = np.asarray(stock)[:ph, :, :, 0].sum(axis=0)
+                acc['tavg_acc'] = t
+            elif isinstance(m, monitors_mod.Bold) and stock is not None:
+                stock = np.asarray(stock)
+                b = np.zeros((stock.shape[0], nvoi, n))
+                b[:, voi] = stock[..., 0]
+                acc['bold_stock'] = b
+                ia = np.zeros((nvoi, n))
+                interim = st.get('monitor_interim_%d' % (k + 1))
+                if interim is not None:
+                    ia[voi] = np.asarray(interim)[..., 0]
+                acc['bold_acc'] = ia
+        self._acc = acc or None
+        if self.integrator.stochastic and st.get('integrator_noise_rng_state_algo') is not None:
+            self.integrator.noise.random_stream.set_state((
+                st['integrator_noise_rng_state_algo'], st['integrator_noise_rng_state_keys'],
+                st['integrator_noise_rng_state_pos'], st['integrator_noise_rng_state_has_gauss'],
+                st['integrator_noise_rng_state_cached_gauss']))
+        return self
 
     def run(self, **kwds):
         """All monitor outputs of one call: [(times, data(T, nvoi, n, 1)), ...]
