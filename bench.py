@@ -240,7 +240,8 @@ def run_serving(args, rank, local):
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     st = srv.stats()
-    bad = sum(1 for r in srv.requests.values() if r.status)
+    bad = [dict(zip(('model', 'regions', 'dt_ms', 'length_ms'), plan[k][1:]), seed=1000 + k, status=r.status)
+           for k, r in sorted(srv.requests.items()) if r.status]
     line = {'metric': 'serving sims/s with p50/p99 latency (continuous batching)', 'value': st['sims_per_s'],
             'unit': 'sims/s', 'n_gpus': 1, 'steps': args.requests, 'warmup': 0, 'ms_per_step': 1e3 * wall / args.requests,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
@@ -251,7 +252,7 @@ def run_serving(args, rank, local):
             'latency_mean_s': st['latency_mean_s'], 'region_steps_per_s': st['region_steps_per_s'],
             'memory_budget_bytes': st['memory_budget_bytes'], 'memory_peak_bytes': st['memory_peak_bytes'],
             'memory_mean_bytes': st['memory_mean_bytes'], 'groups': st['groups'], 'gpu_launches': st['launches'],
-            'nonfinite_requests': bad, 'wall_s': wall}
+            'nonfinite_requests': len(bad), 'nonfinite': bad[:16], 'wall_s': wall}
     if clocks:
         line['clocks'] = clocks
     print(json.dumps(line), flush=True)

@@ -296,6 +296,32 @@ def test_philox_stream_matches_oracle():
     report('philox rww tavg vs oracle', tavg[..., 0], out[0][1], 1e-4)
 
 
+@pytest.mark.parametrize('dt', [0.1, 0.05])
+def test_philox_jansen_rit_partial_noise_matches_oracle(dt):
+    """JansenRit + SigmoidalJansenRit + HeunStochastic with noise on y4 only
+    (the other five variables have sigma 0) driven by the device's Philox
+    stream, 68 regions with the ring in shared memory (the blocked loop's
+    straight-line blocks): equals the oracle fed the same stream, and stays
+    finite."""
+    T = tvb()
+    from tvb_b200 import synthetic
+    w, L = synthetic.connectome(68, 0.30, 10.0, 200.0, seed=3)
+    nsig = np.array([0.0, 0.0, 0.0, 0.0, 1e-5, 0.0])
+    sim = T['Simulator'](model=T['models'].JansenRit(), connectivity=T['Connectivity'](w, L, speed=5.0),
+                         coupling=T['coupling'].SigmoidalJansenRit(),
+                         integrator=T['integrators'].HeunStochastic(dt=dt, noise=T['noise'].Additive(nsig=nsig,
+                                                                                                   noise_seed=7)),
+                         monitors=[T['monitors'].TemporalAverage(period=1.0)], simulation_length=300.0).configure()
+    buf0, st0 = sim.history_buffer[..., 0].copy(), sim.current_state[..., 0].copy()
+    (tt, tavg), = sim.run()
+    assert np.isfinite(tavg).all()
+    n_steps = int(round(300.0 / dt))
+    z = O.philox_normals(7, 0, np.arange(1, n_steps + 1), 6, 68)
+    out, _ = O.simulate('JansenRit', {}, w, L, 5.0, dt, 'SigmoidalJansenRit', {}, 'HeunStochastic', n_steps,
+                        [O.Monitor('TemporalAverage', 1.0)], buf0, st0, 0, nsig=nsig, noise_z=z)
+    report('philox jr (noise on y4) dt %g tavg vs oracle' % dt, tavg[..., 0], out[0][1], 1e-3)
+
+
 @pytest.mark.parametrize('cfun', ['Linear', 'SigmoidalJansenRit', 'Difference'])
 def test_kernel_variants_agree(cfun):
     """The row kernel (rings in shared or global memory), its split form

@@ -729,7 +729,8 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                 }
                 if (act) {
                     if (SchemeTraits<SCHEME>::stoch && zq != (s >> 2)) node.philox_block(i, s, node.zc);
-                    float zn[M::NINT][4];
+                    // variables with a zero sigma draw nothing: their normals stay 0 (0 * z must not see garbage)
+                    float zn[M::NINT][4] = {};
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
                         float c[NCV], z[M::NINT];

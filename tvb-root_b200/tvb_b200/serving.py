@@ -10,9 +10,10 @@ and runs them concurrently:
   when the bytes of its arenas fit in the memory budget and its group has a
   free slot; otherwise it waits (requests behind it that fit are admitted).
 * Groups: admitted requests with the same kernel configuration (model,
-  coupling, scheme, noise kind, dt, observed variables, region count) share
-  one slot table (a device array of ``tvbk_inst`` descriptors) and one CUDA
-  stream.  Each launch advances every occupied slot of a group by one chunk
+  coupling, scheme, noise kind, dt, observed variables, region count and the
+  kernel variant chosen for them) share one slot table (a device array of
+  ``tvbk_inst`` descriptors, allocated on the group's stream) and one CUDA
+  stream; everything a group does on the device is ordered on that stream.  Each launch advances every occupied slot of a group by one chunk
   of steps (``tvbk_sim_run``); a slot whose request finished is inert.  Groups
   run on separate streams, so their launches overlap on the device.
 * Continuous batching: between chunks, finished requests are retired (their
@@ -67,8 +68,11 @@ class _Group:
     def __init__(self, key, device, max_slots):
         self.key = key
         self.stream = torch.cuda.Stream(device=device)
-        self.desc = torch.zeros(max_slots * INST_BYTES, dtype=torch.uint8, device=device)
-        self.status = torch.zeros(max_slots, dtype=torch.int32, device=device)
+        # allocated and zero-filled on the group's own stream: every later use of the slot table (descriptor
+        # writes, launches) is on that stream, so no fill on another stream can land after a descriptor write
+        with torch.cuda.stream(self.stream):
+            self.desc = torch.zeros(max_slots * INST_BYTES, dtype=torch.uint8, device=device)
+            self.status = torch.zeros(max_slots, dtype=torch.int32, device=device)
         self.slots = [None] * max_slots
         self.inflight = collections.deque()   # events of queued chunks
         self.launches = 0
@@ -127,10 +131,13 @@ class SimulationServer:
         spec, noise_kind = sim.instance_spec(int(n_steps), stream=rid)
         if noise_kind == _lib.NOISE_FED:
             raise NotImplementedError('the server draws device noise; use noise_source="philox"')
-        key = (sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, float(np.float32(sim.integrator.dt)),
-               tuple(sim._voi_codes), sim.number_of_nodes)
         plan = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, sim.integrator.dt, sim._voi_codes,
                      [spec], device=self.device, gather='row', allocate=False)
+        # one kernel configuration per group: the components and the variant the plan chose (ring staging,
+        # cluster, prefetch, sigmoid ring), so every occupant of a launch has the buffers that launch reads
+        key = (sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, float(np.float32(sim.integrator.dt)),
+               tuple(sim._voi_codes), sim.number_of_nodes, plan.ring_in_smem, plan.cluster, plan.prefetch,
+               plan.sigma)
         req = _Request(rid, sim, spec, noise_kind, key, plan, time.perf_counter() if t_submit is None else t_submit)
         if req.footprint > self.budget:
             raise ValueError('request needs %d bytes, more than the budget of %d' % (req.footprint, self.budget))
