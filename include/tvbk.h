@@ -120,6 +120,8 @@ typedef struct tvbk_inst {
     const float* noise_fed;      /* [*][nintvar][n] standard normals; step s reads row s - fed_base - 1 */
     /* monitors (NULL disables one) */
     float* raw;                  /* [*][nvoi][n]; step s writes row s - raw_base - 1 */
+    float* sub;                  /* [*][nvoi][n] the state at every step s with s % sub_istep == 0 (SubSample,
+                                  * and GlobalAverage / SpatialAverage reduce it): row s / sub_istep - sub_base - 1 */
     float* tavg;                 /* [*][nvoi][n]; sample s / tavg_istep - tavg_base - 1 */
     float* tavg_acc;             /* [nvoi][n] running sum of the current period */
     double* bold;                /* [*][nvoi][n]; sample s / bold_istep - bold_base - 1 */
@@ -128,9 +130,9 @@ typedef struct tvbk_inst {
     const double* hrf;           /* [stock_len] reversed haemodynamic kernel */
     int64_t step;                /* last completed step (the reference's current_step) */
     int64_t step_end;            /* run until step == step_end */
-    int64_t raw_base, fed_base, tavg_base, bold_base;
+    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base;
     int32_t n, nnz, horizon, ring_len;
-    int32_t tavg_istep, bold_istep, bold_ii, stock_len;
+    int32_t tavg_istep, bold_istep, bold_ii, stock_len, sub_istep;
     float cfun[6];               /* coupling parameters, see tvbk_sim_run */
     uint32_t seed, stream;       /* Philox key */
     double bold_k1v0;            /* k_1 * V_0 of the FirstOrderVolterra kernel */

@@ -333,8 +333,8 @@ def iround(x):
 
 
 class Monitor:
-    def __init__(self, kind, period=None, voi=None):
-        self.kind, self.period, self.voi = kind, period, voi
+    def __init__(self, kind, period=None, voi=None, spatial_mask=None):
+        self.kind, self.period, self.voi, self.spatial_mask = kind, period, voi, spatial_mask
 
 
 def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, coupling_params,
@@ -417,6 +417,14 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
         elif m.kind == 'TemporalAverage':
             st['istep'] = iround(m.period / dt)
             st['stock'] = np.zeros((st['istep'], len(mv), X.shape[1]))
+        elif m.kind in ('SubSample', 'GlobalAverage', 'SpatialAverage'):
+            st['istep'] = iround(m.period / dt)
+            if m.kind == 'SpatialAverage':                # monitors.py:311-318
+                nn = X.shape[1]
+                total = np.zeros((nn, int(m.spatial_mask.max()) + 1))
+                total[np.arange(nn), m.spatial_mask] = 1
+                total = total.T
+                st['mean'] = total / np.sum(total, axis=1)[:, np.newaxis]
         elif m.kind == 'Bold':
             st['istep'] = iround(m.period / dt)
             st['ii'] = int(round((1.0 / 2.0 ** -2) / dt))
@@ -481,6 +489,15 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
                 if step % st['istep'] == 0:
                     st['t'].append((step - st['istep'] / 2.0) * dt)
                     st['y'].append(np.mean(st['stock'], axis=0))
+            elif m.kind in ('SubSample', 'GlobalAverage', 'SpatialAverage'):
+                if step % st['istep'] == 0:
+                    st['t'].append(step * dt)
+                    if m.kind == 'SubSample':              # monitors.py:219-222
+                        st['y'].append(o.copy())
+                    elif m.kind == 'GlobalAverage':        # monitors.py:350-355
+                        st['y'].append(np.mean(o, axis=1)[:, np.newaxis])
+                    else:                                  # monitors.py:321-325 (o is (nvoi, n): no modes axis)
+                        st['y'].append(np.dot(st['mean'], o.T).T)
             elif m.kind == 'Bold':                       # monitors.py:942-962
                 ii = st['ii']
                 st['interim'][(step % ii) - 1] = o

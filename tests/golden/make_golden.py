@@ -497,6 +497,45 @@ def case_couplings(R):
     save('couplings_40', **out)
 
 
+def case_monitors(R):
+    """SubSample, GlobalAverage and SpatialAverage (period 1 ms) beside Raw and
+    TemporalAverage: Generic2dOscillator, the 40-region connectome of
+    case_couplings, Linear a=0.0152, HeunDeterministic dt 0.1, 40 ms; and the
+    same monitors on ReducedWongWang with EulerStochastic (reference noise)."""
+    w, L = synthetic_connectome(40, 0.40, 10.0, 120.0, seed=21)
+    speed = 3.0
+    mask = np.arange(40) % 3
+    M = R['monitors']
+
+    def mons():
+        return [M.SubSample(period=1.0), M.GlobalAverage(period=1.0),
+                M.SpatialAverage(period=1.0, spatial_mask=mask), M.TemporalAverage(period=1.0)]
+
+    def build():
+        return R['simulator'].Simulator(
+            model=R['models'].Generic2dOscillator(), connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].Linear(a=np.array([0.0152])),
+            integrator=R['integrators'].HeunDeterministic(dt=0.1), monitors=mons(), simulation_length=40.0)
+    sim, cfg, res, _, _ = run_sim(R, build, 40.0, False, ic_seed=204)
+    out = dict(weights=w, tract_lengths=L, speed=speed, spatial_mask=mask, ic_seed=204,
+               g2d_buffer0=cfg['buffer0'], g2d_state0=cfg['state0'])
+    for name, (t, y) in zip(('sub', 'glob', 'spat', 'tavg'), res):
+        out['g2d_%s' % name] = y[..., 0]
+        out['g2d_%s_t' % name] = t
+
+    def build_rww():
+        return R['simulator'].Simulator(
+            model=R['models'].ReducedWongWang(), connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].Linear(a=np.array([0.3])),
+            integrator=R['integrators'].EulerStochastic(dt=0.1, noise=R['noise'].Additive(nsig=np.array([1e-3]))),
+            monitors=mons(), simulation_length=40.0)
+    sim, cfg, res, rec, _ = run_sim(R, build_rww, 40.0, False, record_noise=True)
+    out.update(rww_buffer0=cfg['buffer0'], rww_state0=cfg['state0'], rww_noise_sha256=rec.h.hexdigest())
+    for name, (t, y) in zip(('sub', 'glob', 'spat', 'tavg'), res):
+        out['rww_%s' % name] = y[..., 0]
+    save('monitors_40', **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference/tvb_library')
@@ -524,6 +563,7 @@ def main():
         'rww_full': lambda: case_rww(R, 'rww_68_full', [(16, 16), (31, 8)], 60000.0, False),
         'jr': lambda: case_jr(R),
         'couplings': lambda: case_couplings(R),
+        'monitors': lambda: case_monitors(R),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only:

@@ -441,3 +441,35 @@ def test_epileptor_hyperbolic_tangent_vs_reference():
     np.testing.assert_array_equal(sim.history_buffer[..., 0], fx['epi_tanh_buffer0'])
     (t, tavg), = sim.run()
     report('epileptor tanh tavg vs reference', tavg[..., 0], fx['epi_tanh_tavg'], 1e-4)
+
+
+@pytest.mark.parametrize('which', ['g2d', 'rww'])
+def test_subsample_global_spatial_average_vs_reference(which):
+    """SubSample, GlobalAverage, SpatialAverage and TemporalAverage (period 1 ms) on the device against the
+    reference's runs (G2D deterministic; RWW with the reference's own noise stream)."""
+    T = tvb()
+    fx = G.load('monitors_40')
+    M = T['monitors']
+    mons = [M.SubSample(period=1.0), M.GlobalAverage(period=1.0),
+            M.SpatialAverage(period=1.0, spatial_mask=fx['spatial_mask']), M.TemporalAverage(period=1.0)]
+    conn = T['Connectivity'](weights=fx['weights'], tract_lengths=fx['tract_lengths'], speed=float(fx['speed']))
+    if which == 'g2d':
+        np.random.seed(int(fx['ic_seed']))
+        sim = T['Simulator'](model=T['models'].Generic2dOscillator(), connectivity=conn,
+                             coupling=T['coupling'].Linear(a=0.0152),
+                             integrator=T['integrators'].HeunDeterministic(dt=0.1), monitors=mons,
+                             simulation_length=40.0).configure()
+    else:
+        sim = T['Simulator'](model=T['models'].ReducedWongWang(), connectivity=conn,
+                             coupling=T['coupling'].Linear(a=0.3),
+                             integrator=T['integrators'].EulerStochastic(dt=0.1, noise=T['noise'].Additive(
+                                 nsig=[1e-3])), monitors=mons, simulation_length=40.0,
+                             noise_source='reference').configure()
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx[which + '_buffer0'])
+    res = sim.run()
+    for (t, y), name in zip(res, ('sub', 'glob', 'spat', 'tavg')):
+        ref = fx['%s_%s' % (which, name)]
+        assert y[..., 0].shape == ref.shape, name
+        if which == 'g2d':
+            np.testing.assert_allclose(t, fx['g2d_%s_t' % name], rtol=0, atol=1e-12)
+        report('%s %s vs reference' % (which, name), y[..., 0], ref, 1e-4)

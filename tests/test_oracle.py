@@ -219,3 +219,27 @@ def test_epileptor_hyperbolic_tangent_two_cvars():
     ref = fx['epi_tanh_tavg']
     err = np.abs(out[0][1] - ref).max() / np.abs(ref).max()
     assert err < 1e-9, err
+
+
+def test_subsample_global_spatial_average_monitors():
+    """SubSample, GlobalAverage, SpatialAverage (monitors.py:213-360) against reference runs (G2D, and RWW
+    with the reference's own noise stream)."""
+    fx = G.load('monitors_40')
+    w, L = fx['weights'], fx['tract_lengths']
+    mask = fx['spatial_mask']
+    mons = [O.Monitor('SubSample', 1.0), O.Monitor('GlobalAverage', 1.0),
+            O.Monitor('SpatialAverage', 1.0, spatial_mask=mask), O.Monitor('TemporalAverage', 1.0)]
+    out, _ = O.simulate('Generic2dOscillator', {}, w, L, float(fx['speed']), 0.1, 'Linear', {'a': 0.0152},
+                        'HeunDeterministic', 400, mons, fx['g2d_buffer0'], fx['g2d_state0'], 0)
+    for (t, y), name in zip(out, ('sub', 'glob', 'spat', 'tavg')):
+        ref = fx['g2d_' + name]
+        assert y.shape == ref.shape, name
+        np.testing.assert_allclose(t, fx['g2d_%s_t' % name], rtol=0, atol=1e-12)
+        assert np.abs(y - ref).max() / np.abs(ref).max() < 1e-9, name
+    H = fx['rww_buffer0'].shape[0]
+    z = O.reference_noise(42, [O.MODEL_INFO['ReducedWongWang']['ranges']['S']], H, 40, 1, 400)
+    out, _ = O.simulate('ReducedWongWang', {}, w, L, float(fx['speed']), 0.1, 'Linear', {'a': 0.3},
+                        'EulerStochastic', 400, mons, fx['rww_buffer0'], fx['rww_state0'], 0, nsig=[1e-3], noise_z=z)
+    for (t, y), name in zip(out, ('sub', 'glob', 'spat', 'tavg')):
+        ref = fx['rww_' + name]
+        assert np.abs(y - ref).max() / np.abs(ref).max() < 1e-9, name

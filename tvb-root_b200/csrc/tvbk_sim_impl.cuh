@@ -275,10 +275,11 @@ struct Node {
     const float* fed_p;
     float* tavg_p;
     double* bold_p;
-    int ph_t, ph_b, ph_i, q_prev;
+    float* sub_p;
+    int ph_t, ph_b, ph_i, ph_s, q_prev;
     // descriptor fields used every step, held in registers: read through the
     // descriptor pointer they would be reloaded after every store
-    int t_istep, b_istep, b_ii, SL;
+    int t_istep, b_istep, b_ii, SL, s_istep;
     double* stock;
     const double* hrf;
     double k1v0;
@@ -306,6 +307,7 @@ struct Node {
         t_istep = Ip->tavg_istep;
         b_istep = Ip->bold_istep;
         b_ii = Ip->bold_ii;
+        s_istep = Ip->sub_istep;
         SL = Ip->stock_len;
         stock = Ip->bold_stock;
         hrf = Ip->hrf;
@@ -317,6 +319,8 @@ struct Node {
         ph_b = do_bold ? (int)(s0 % Ip->bold_istep) : 0;
         ph_i = do_bold ? (int)(s0 % Ip->bold_ii) : 0;
         q_prev = do_bold ? (int)((s0 / Ip->bold_ii) % Ip->stock_len) : 0;
+        ph_s = Ip->sub ? (int)(s0 % Ip->sub_istep) : 0;
+        sub_p = Ip->sub ? Ip->sub + (size_t)(s0 / Ip->sub_istep - Ip->sub_base) * nvoi * n + i : nullptr;
         raw_p = Ip->raw ? Ip->raw + (size_t)(s0 - Ip->raw_base) * nvoi * n + i : nullptr;
         fed_p = Ip->noise_fed ? Ip->noise_fed + (size_t)(s0 - Ip->fed_base) * NINT * n + i : nullptr;
         tavg_p = do_tavg ? Ip->tavg + (size_t)(s0 / Ip->tavg_istep - Ip->tavg_base) * nvoi * n + i : nullptr;
@@ -462,6 +466,13 @@ struct Node {
                 bold_p += (size_t)nvoi * n;
             }
         }
+        if (sub_p != nullptr && ++ph_s == s_istep) {
+            ph_s = 0;
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) sub_p[v * n] = M::observe(L.voi[v], x);
+            sub_p += (size_t)nvoi * n;
+        }
     }
 
     // ---- pieces of a step for the row kernel's blocked loop ----------------
@@ -471,15 +482,18 @@ struct Node {
     // the CTA (active or not) keeps the same clock and the kernel's control
     // flow can branch on it uniformly.
     static constexpr int kBigCount = 1 << 30;
-    int cd_t, cd_i, cd_b;
-    bool on_t, on_b;
+    int cd_t, cd_i, cd_b, cd_s;
+    bool on_t, on_b, on_s;
 
     __device__ __forceinline__ void init_clock(const tvbk_inst* Ip, int64_t s0) {
         t_istep = Ip->tavg_istep;
         b_istep = Ip->bold_istep;
         b_ii = Ip->bold_ii;
+        s_istep = Ip->sub_istep;
         on_t = Ip->tavg != nullptr;
         on_b = Ip->bold != nullptr;
+        on_s = Ip->sub != nullptr;
+        cd_s = on_s ? Ip->sub_istep - (int)(s0 % Ip->sub_istep) : kBigCount;
         cd_t = on_t ? Ip->tavg_istep - (int)(s0 % Ip->tavg_istep) : kBigCount;
         cd_i = on_b ? Ip->bold_ii - (int)(s0 % Ip->bold_ii) : kBigCount;
         cd_b = on_b ? Ip->bold_istep - (int)(s0 % Ip->bold_istep) : kBigCount;
@@ -509,7 +523,8 @@ struct Node {
     // Advance the clock by m steps, the last of which is step s, and take the
     // samples that fall on step s (every thread calls it; `act` threads write).
     // m > 1 only when no sample falls on the m - 1 steps before s.
-    __device__ __forceinline__ void tick(int m, bool act, int64_t s, int i, int n, int nvoi) {
+    __device__ __forceinline__ void tick(const tvbk_launch& L, int m, bool act, int64_t s, int i, int n) {
+        const int nvoi = L.nvoi;
         if (on_t) cd_t -= m;
         if (cd_t == 0) {
             cd_t = t_istep;
@@ -544,6 +559,16 @@ struct Node {
         if (cd_b == 0) {
             cd_b = b_istep;
             if (act) bold_sample(s, i, n, nvoi);
+        }
+        if (on_s) cd_s -= m;
+        if (cd_s == 0) {
+            cd_s = s_istep;
+            if (act) {
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) sub_p[v * n] = M::observe(L.voi[v], x);
+                sub_p += (size_t)nvoi * n;
+            }
         }
     }
 
@@ -712,7 +737,6 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         // block, blocks with a sample inside, fed noise, a barrier interval
         // below 4) runs one at a time.  Both paths do the same arithmetic.
         node.init_clock(Ip, s0);
-        const int nvoi = L.nvoi;
         const bool fed = L.noise == TVBK_NOISE_FED;
         int64_t zq = -1;  // Philox block whose normals are in node.zc
         float cnext[NCV];
@@ -721,7 +745,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         int ks = 0;
         while (ks < nsteps) {
             const bool fast = !fed && K >= 4 && (s & 3) == 0 && nsteps - ks >= 4 && node.cd_t >= 4 &&
-                              node.cd_i >= 4 && node.cd_b >= 4;  // uniform over the CTA
+                              node.cd_i >= 4 && node.cd_b >= 4 && node.cd_s >= 4;  // uniform over the CTA
             if (fast) {
                 if (since_sync + 4 > K) {
                     since_sync = 0;
@@ -756,7 +780,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                     for (int r = 0; r < 4; ++r) wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
                 }
                 zq = (s >> 2) + 1;
-                node.tick(4, act, s + 3, i, n, nvoi);
+                node.tick(L, 4, act, s + 3, i, n);
                 since_sync += 4;
                 s += 4;
                 ks += 4;
@@ -775,7 +799,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                     write(wslot);
                 }
                 zq = s >> 2;
-                node.tick(1, act, s, i, n, nvoi);
+                node.tick(L, 1, act, s, i, n);
                 if (++since_sync == K) {
                     since_sync = 0;
                     __syncthreads();

@@ -48,6 +48,7 @@ class Inst(ctypes.Structure):
         ('noise_sigma', ctypes.c_void_p),
         ('noise_fed', ctypes.c_void_p),
         ('raw', ctypes.c_void_p),
+        ('sub', ctypes.c_void_p),
         ('tavg', ctypes.c_void_p),
         ('tavg_acc', ctypes.c_void_p),
         ('bold', ctypes.c_void_p),
@@ -60,6 +61,7 @@ class Inst(ctypes.Structure):
         ('fed_base', ctypes.c_int64),
         ('tavg_base', ctypes.c_int64),
         ('bold_base', ctypes.c_int64),
+        ('sub_base', ctypes.c_int64),
         ('n', ctypes.c_int32),
         ('nnz', ctypes.c_int32),
         ('horizon', ctypes.c_int32),
@@ -68,6 +70,7 @@ class Inst(ctypes.Structure):
         ('bold_istep', ctypes.c_int32),
         ('bold_ii', ctypes.c_int32),
         ('stock_len', ctypes.c_int32),
+        ('sub_istep', ctypes.c_int32),
         ('cfun', ctypes.c_float * 6),
         ('seed', ctypes.c_uint32),
         ('stream', ctypes.c_uint32),

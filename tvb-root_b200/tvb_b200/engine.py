@@ -93,7 +93,7 @@ class InstanceSpec:
     """
 
     def __init__(self, conn, ring0, state0, params, cfun, n_steps, step0=0, sigma=None, noise_fed=None,
-                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None):
+                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0):
         self.conn = conn
         self.ring0 = ring0
         self.state0 = state0
@@ -108,6 +108,7 @@ class InstanceSpec:
         self.raw = raw
         self.tavg_istep = int(tavg_istep)
         self.bold = bold
+        self.sub_istep = int(sub_istep)  # SubSample / GlobalAverage / SpatialAverage period in steps (0: none)
         # monitor accumulators carried over from a previous run of the same
         # simulation: dict with 'tavg_acc' (nvoi, n), 'bold_acc' (nvoi, n),
         # 'bold_stock' (stock_len, nvoi, n); None starts them at zero
@@ -350,6 +351,9 @@ class Batch:
                 bi = s.bold['istep']
                 m['bold_rows'] = s1 // bi - s.step0 // bi
                 outa.add(('bold', k), max(m['bold_rows'], 1) * nvoi * n * 8)
+            if s.sub_istep:
+                m['sub_rows'] = s1 // s.sub_istep - s.step0 // s.sub_istep
+                outa.add(('sub', k), max(m['sub_rows'], 1) * nvoi * n * 4)
             self.meta.append(m)
         init.add(('insts',), len(specs) * _lib.INST_DTYPE.itemsize)
         zero.add(('status',), len(specs) * 4)
@@ -423,6 +427,10 @@ class Batch:
                     if (key, k) in init.regions and s.acc0.get(key) is not None:
                         put((key, k), np.asarray(s.acc0[key], dtype=dtype))
             d['raw'] = zaddr(('raw', k))
+            d['sub'] = zaddr(('sub', k))
+            if s.sub_istep:
+                d['sub_istep'] = s.sub_istep
+                d['sub_base'] = s.step0 // s.sub_istep
             d['tavg'] = zaddr(('tavg', k))
             d['tavg_acc'] = zaddr(('tavg_acc', k))
             d['bold'] = zaddr(('bold', k))
@@ -573,6 +581,8 @@ class Batch:
             out['tavg'] = self._oview(('tavg', k), torch.float32, (m['tavg_rows'], nvoi, m['n']))
         if 'bold_rows' in m:
             out['bold'] = self._oview(('bold', k), torch.float64, (m['bold_rows'], nvoi, m['n']))
+        if 'sub_rows' in m:
+            out['sub'] = self._oview(('sub', k), torch.float32, (m['sub_rows'], nvoi, m['n']))
         return out
 
     def outputs_host(self):
@@ -586,7 +596,7 @@ class Batch:
             o = {}
             nvoi, n = self.nvoi, m['n']
             for key, dt, rows in (('raw', np.float32, 'raw_rows'), ('tavg', np.float32, 'tavg_rows'),
-                                  ('bold', np.float64, 'bold_rows')):
+                                  ('bold', np.float64, 'bold_rows'), ('sub', np.float32, 'sub_rows')):
                 if rows in m:
                     off, nb = self.out.regions[(key, k)]
                     cnt = m[rows] * nvoi * n

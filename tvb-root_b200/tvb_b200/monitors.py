@@ -103,4 +103,55 @@ class Bold(Monitor):
         return steps * self.dt
 
 
-MONITORS = {cls.__name__: cls for cls in (Raw, TemporalAverage, Bold)}
+class SubSample(Monitor):
+    """The variables of interest at every step with step % istep == 0,
+    stamped step * dt (monitors.py:213-222)."""
+
+    def times(self, steps):
+        return steps * self.dt
+
+    def reduce(self, y):
+        """(T, nvoi, n) sampled states -> this monitor's data."""
+        return y
+
+
+class GlobalAverage(SubSample):
+    """Mean over all regions of the sub-sampled variables of interest,
+    (T, nvoi, 1) (monitors.py:342-360)."""
+
+    def reduce(self, y):
+        return y.astype(np.float64).mean(axis=2)[:, :, None]
+
+
+class SpatialAverage(SubSample):
+    """Mean over each group of regions of the sub-sampled variables of
+    interest; spatial_mask gives each region's group, a contiguous set of
+    indices from 0 (monitors.py:231-326).  (T, nvoi, groups)."""
+
+    def __init__(self, period=None, variables_of_interest=None, spatial_mask=None):
+        super().__init__(period, variables_of_interest)
+        if spatial_mask is None:
+            raise NotImplementedError('SpatialAverage on the device needs an explicit spatial_mask')
+        self.spatial_mask = np.asarray(spatial_mask, dtype=int)
+
+    def config_for_sim(self, sim):
+        super().config_for_sim(sim)
+        n = sim.number_of_nodes
+        if self.spatial_mask.size != n:
+            raise ValueError('spatial_mask must be a vector of length number_of_nodes.')
+        areas = np.unique(self.spatial_mask)
+        if not np.all(areas == np.arange(len(areas))):
+            raise ValueError('Areas in the spatial_mask must be specified as a contiguous set of indices '
+                             'starting from zero.')
+        total = np.zeros((n, len(areas)))
+        total[np.arange(n), self.spatial_mask] = 1
+        total = total.T
+        self.spatial_mean = total / total.sum(axis=1)[:, None]
+        return self
+
+    def reduce(self, y):
+        # numpy.dot(spatial_mean, state[voi]) per sample, (groups, nvoi) -> (nvoi, groups)
+        return np.einsum('gn,tvn->tvg', self.spatial_mean, y.astype(np.float64))
+
+
+MONITORS = {cls.__name__: cls for cls in (Raw, TemporalAverage, Bold, SubSample, GlobalAverage, SpatialAverage)}

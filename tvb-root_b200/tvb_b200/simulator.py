@@ -86,6 +86,11 @@ def adopt_monitor(mon):
         return monitors_mod.Raw()
     if name == 'TemporalAverage':
         return monitors_mod.TemporalAverage(period=mon.period, variables_of_interest=voi)
+    if name in ('SubSample', 'GlobalAverage'):
+        return monitors_mod.MONITORS[name](period=mon.period, variables_of_interest=voi)
+    if name == 'SpatialAverage':
+        return monitors_mod.SpatialAverage(period=mon.period, variables_of_interest=voi,
+                                           spatial_mask=getattr(mon, 'spatial_mask', None))
     if name == 'Bold':
         if type(mon.hrf_kernel).__name__ != 'FirstOrderVolterra':
             raise NotImplementedError('Bold on the device supports the FirstOrderVolterra kernel')
@@ -226,8 +231,11 @@ class Simulator:
         raw = any(isinstance(m, monitors_mod.Raw) for m in self.monitors)
         tavg = [m for m in self.monitors if isinstance(m, monitors_mod.TemporalAverage)]
         bold = [m for m in self.monitors if isinstance(m, monitors_mod.Bold)]
-        if len(set(m.istep for m in tavg)) > 1 or len(set(m.istep for m in bold)) > 1:
+        sub = [m for m in self.monitors if isinstance(m, monitors_mod.SubSample)]
+        if len(set(m.istep for m in tavg)) > 1 or len(set(m.istep for m in bold)) > 1 or \
+                len(set(m.istep for m in sub)) > 1:
             raise NotImplementedError('monitors of one kind must share their period')
+        self._sub_istep = sub[0].istep if sub else 0
         bspec = None
         if bold:
             b = bold[0]
@@ -254,7 +262,7 @@ class Simulator:
                             self.coupling.kernel_params(), n_steps, step0=self.current_step, sigma=self._sigma,
                             noise_fed=fed, seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                             stream=self.stream_id if stream is None else stream, raw=raw, tavg_istep=tavg_istep,
-                            bold=bspec)
+                            bold=bspec, sub_istep=self._sub_istep)
         if self._acc is not None:
             spec.acc0 = self._acc
         return spec, noise_kind
@@ -286,6 +294,9 @@ class Simulator:
             elif isinstance(m, monitors_mod.TemporalAverage):
                 st = steps[steps % m.istep == 0]
                 t, y = m.times(st.astype(np.float64)), out['tavg'][:, m.voi]
+            elif isinstance(m, monitors_mod.SubSample):
+                st = steps[steps % m.istep == 0]
+                t, y = m.times(st.astype(np.float64)), m.reduce(out['sub'][:, m.voi])
             else:
                 st = steps[steps % m.istep == 0]
                 t, y = m.times(st.astype(np.float64)), out['bold'][:, m.voi]

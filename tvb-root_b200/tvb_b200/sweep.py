@@ -107,7 +107,7 @@ class ParameterSweep:
             spec = InstanceSpec(conn, sim.history_buffer[..., 0], sim.current_state[..., 0], params, cf,
                                 int(self.n_steps_each[i]), step0=sim.current_step, sigma=sigma, noise_fed=None,
                                 seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
-                                stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec)
+                                stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep)
             specs.append(spec)
         self._specs = specs
         noise_kind = _lib.NOISE_NONE
@@ -175,7 +175,7 @@ class ParameterSweep:
         if fc and any(isinstance(m, monitors_mod.Bold) for m in self.monitors):
             res['fc'] = self.fc_device().cpu().numpy()
         outs = self.batch.outputs_host()
-        for key in ('raw', 'tavg', 'bold'):
+        for key in ('raw', 'tavg', 'bold', 'sub'):
             if key in outs[0]:
                 arrs = [o[key] for o in outs]
                 # instances of uneven lengths give a list of (T_i, nvoi, n) arrays
