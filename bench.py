@@ -131,9 +131,15 @@ def _oracle_worker(args):
     hist = O.reference_initial_history(rs, [info['ranges']['S']], H, N_REGIONS)
     t0 = time.perf_counter()
     z = rs.normal(size=(n_steps, 1, N_REGIONS))
-    O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic', n_steps,
-               [O.Monitor('Bold', 2000.0)], hist[:, [0]].astype(np.float32), hist[0], 0, nsig=[nsig], noise_z=z)
-    return time.perf_counter() - t0
+    out, fin = O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic', n_steps,
+                          [O.Monitor('Bold', 2000.0)], hist[:, [0]].astype(np.float32), hist[0], 0, nsig=[nsig],
+                          noise_z=z)
+    el = time.perf_counter() - t0
+    # the all-float64 variant of the same run (float64 history and weights), untimed: the error reference
+    out64, fin64 = O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic',
+                              n_steps, [O.Monitor('Bold', 2000.0)], hist[:, [0]], hist[0], 0, nsig=[nsig],
+                              noise_z=z, history_dtype=np.float64)
+    return el, dict(bold=out[0][1], state=fin['state'], bold64=out64[0][1], state64=fin64['state'])
 
 
 def cpu_baseline(n_steps=20000, cores=None):
@@ -144,13 +150,65 @@ def cpu_baseline(n_steps=20000, cores=None):
     ctx = mp.get_context('spawn')
     t0 = time.perf_counter()
     with ctx.Pool(cores) as pool:
-        times = pool.map(_oracle_worker, [(k, n_steps, G[i], S[i]) for k, i in enumerate(pick)])
+        res = pool.map(_oracle_worker, [(k, n_steps, G[i], S[i]) for k, i in enumerate(pick)])
     wall = time.perf_counter() - t0
+    times = [r[0] for r in res]
     rs = cores * n_steps * N_REGIONS
-    return {'value': rs / max(times), 'unit': UNIT, 'cores': cores, 'kind': 'port',
-            'sample': '%d RWW sweep instances (one per core), %d steps (%g ms) each, oracle numpy path '
-                      'incl. per-step noise draws; value = instances x steps x regions / slowest instance'
-                      % (cores, n_steps, n_steps * DT), 'wall_s': wall}
+    cb = {'value': rs / max(times), 'unit': UNIT, 'cores': cores, 'kind': 'port',
+          'sample': '%d RWW sweep instances (one per core), %d steps (%g ms) each, oracle numpy path '
+                    'incl. per-step noise draws; value = instances x steps x regions / slowest instance'
+                    % (cores, n_steps, n_steps * DT), 'wall_s': wall}
+    # kept for the error check against the device (not part of the reported baseline)
+    cb['_check'] = dict(points=pick, n_steps=n_steps, outputs=[r[1] for r in res])
+    return cb
+
+
+def error_vs_oracle(check):
+    """The device's float32 run of the CPU-baseline instances, fed the same
+    RandomState normals, against the oracle: the all-float64 variant and the
+    stock (float32 ring) variant.  Relative errors of the final state and of
+    the Bold sample, max over the instances."""
+    import torch
+    from oracle import tvb_oracle as O
+    from tvb_b200 import _lib, synthetic
+    from tvb_b200.engine import Batch
+    sw = make_sweep(1, check['n_steps'] * DT).configure()
+    sim = sw._sim
+    G, S = sweep_grid()
+    n_steps = check['n_steps']
+    rs = np.random.RandomState(42)
+    H = sim._conn.horizon
+    info = O.MODEL_INFO['ReducedWongWang']
+    hist = O.reference_initial_history(rs, [info['ranges']['S']], H, N_REGIONS)
+    z = rs.normal(size=(n_steps, 1, N_REGIONS)).astype(np.float32)
+    specs = []
+    for k, i in enumerate(check['points']):
+        spec, _ = sim.instance_spec(n_steps)
+        spec.ring0 = hist[:, [0]].astype(np.float32)
+        spec.state0 = hist[0]
+        spec.cfun = [float(G[i]), 0.0]
+        from tvb_b200.simulator import noise_sigma
+        spec.sigma = noise_sigma(np.array([S[i]]), 1, N_REGIONS, DT)
+        spec.noise_fed = z
+        specs.append(spec)
+    b = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, _lib.NOISE_FED, DT, sim._voi_codes, specs)
+    b.run()
+    outs = b.outputs_host()
+    err = {}
+    for tag, bkey, skey in (('fp64', 'bold64', 'state64'), ('stock', 'bold', 'state')):
+        bm, sm, srms = 0.0, 0.0, 0.0
+        for k, ref in enumerate(check['outputs']):
+            bo = outs[k]['bold'][:, 0]
+            rb = np.asarray(ref[bkey])
+            bm = max(bm, float(np.abs(bo - rb).max() / np.abs(rb).max()))
+            st = b.state(k)[0]
+            rsx = np.asarray(ref[skey])[0]
+            d = st - rsx
+            sm = max(sm, float(np.abs(d).max() / np.abs(rsx).max()))
+            srms = max(srms, float(np.sqrt(np.mean(d ** 2)) / np.sqrt(np.mean(rsx ** 2))))
+        err[tag] = {'bold_max_rel': bm, 'state_max_rel': sm, 'state_rms_rel': srms}
+    return {'instances': len(specs), 'steps': n_steps, 'noise': 'the oracle\'s RandomState normals fed to the '
+            'device', 'vs_all_fp64_oracle': err['fp64'], 'vs_stock_oracle': err['stock']}
 
 
 # ------------------------------------------------------------ plain form
@@ -317,6 +375,7 @@ def run_reference(args, rank):
     if rank != 0:
         return
     cb = cpu_baseline(n_steps=args.cpu_steps)
+    cb.pop('_check')
     ms = 1e3 * cb['cores'] * args.cpu_steps * N_REGIONS / cb['value']
     line = {'metric': METRIC, 'value': cb['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
@@ -439,6 +498,10 @@ def main():
     if not e2e_times:
         e2e_times = [float('inf')]
     plain = plain_form(args.plain_steps, rank, args.gather) if args.plain_steps > 0 else None
+    errs = None
+    if cb is not None:
+        check = cb.pop('_check')
+        errs = error_vs_oracle(check)
 
     if world > 1:
         tt = torch.tensor([t_dev, t_kern, float(np.median(e2e_times))], device='cuda', dtype=torch.float64)
@@ -492,6 +555,8 @@ def main():
         if plain:
             plain['batched_over_plain'] = value / plain['value']
             line['plain_single_instance'] = plain
+        if errs:
+            line['error_vs_fp64_oracle'] = errs
         if cb:
             line['cpu_baseline'] = cb
         print(json.dumps(line), flush=True)
