@@ -27,6 +27,8 @@
  *                          (SparseHistory.query_sparse, the delayed-state gather alone)
  *   tvbk_fc                tvb_framework/tvb/adapters/analyzers/cross_correlation_adapter.py:348-380
  *                          (numpy.corrcoef over the Bold time series, per instance)
+ *   tvbk_balloon           tvb_library/tvb/analyzers/fmri_balloon.py:198-364
+ *                          (BalloonModel.evaluate: Balloon-Windkessel BOLD, float64)
  */
 #ifndef TVBK_H
 #define TVBK_H
@@ -240,6 +242,15 @@ int tvbk_gather_delayed(const tvbk_inst* inst_host, int32_t ncvar, int64_t step,
  * (instance-major), fc is [n_inst][n][n] float64.  Rows with zero variance
  * give NaN like numpy.corrcoef. */
 int tvbk_fc(const double* x, int32_t n_inst, int32_t T, int32_t n, double* fc, void* stream);
+
+/* Balloon-Windkessel BOLD of neural-activity series, float64
+ * (tvb_library/tvb/analyzers/fmri_balloon.py:198-364, BalloonModel.evaluate with the
+ * HeunDeterministic scheme).  x and bold are device arrays [T][nseries] (series fastest);
+ * dt in seconds; params (host) = {tau_s, tau_f, tau_o, alpha, E0, V0, k1, k2, k3};
+ * nonlinear = 1 for the non-linear BOLD equation, 0 for the linear one.  Every series
+ * starts from s = 0, f = v = q = 1; bold[0] is the signal of that state. */
+int tvbk_balloon(const double* x, int32_t T, int64_t nseries, double dt, const double* params, int32_t nonlinear,
+                 double* bold, void* stream);
 
 /* Bytes of device scratch that tvbk_sim_run_static keeps inside the library (per GPU). */
 #define TVBK_STATIC_SCRATCH_BYTES (8 * 1024 * 1024)

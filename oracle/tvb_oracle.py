@@ -519,3 +519,40 @@ def functional_connectivity(bold):
     (tvb_framework/tvb/adapters/analyzers/cross_correlation_adapter.py:378):
     numpy.corrcoef(data.T) for data of shape (T, n)."""
     return np.corrcoef(np.asarray(bold, dtype=np.float64).T)
+
+
+# ----------------------------------------------------------------------------
+# Balloon-Windkessel BOLD (analyzer)
+
+
+def balloon_bold(x, dt, tau_s=1.54, tau_f=1.44, tau_o=0.98, alpha=0.32, E0=0.4, V0=4.0, k=(None, None, None),
+                 nonlinear=True):
+    """BalloonModel.evaluate after its input transformation
+    (tvb/analyzers/fmri_balloon.py:215-283,339-364): x (T, n) float64 neural
+    input, dt in seconds, HeunDeterministic from s = 0, f = v = q = 1;
+    returns the BOLD signal (T, n), step 0 included."""
+    k1, k2, k3 = k
+    T = x.shape[0]
+    y = np.zeros((4, x.shape[1]))
+    y[1:] = 1.0
+
+    def dfun(y, xt):
+        s, f, v, q = y
+        return np.array([xt - (1. / tau_s) * s - (1. / tau_f) * (f - 1), s,
+                         (1. / tau_o) * (f - v ** (1. / alpha)),
+                         (1. / tau_o) * ((f * (1. - (1. - E0) ** (1. / f)) / E0) - (v ** (1. / alpha)) * (q / v))])
+
+    def bold(y):
+        v, q = y[2], y[3]
+        if nonlinear:
+            return V0 * (k1 * (1. - q) + k2 * (1. - q / v) + k3 * (1. - v))
+        return V0 * ((k1 + k2) * (1. - q) + (k3 - k2) * (1. - v))
+
+    out = np.zeros((T, x.shape[1]))
+    out[0] = bold(y)
+    for t in range(1, T):
+        m0 = dfun(y, x[t])
+        inter = y + dt * (m0 + 0.0)                          # integrators.py:310
+        y = y + (m0 + dfun(inter, x[t])) * dt / 2.0          # integrators.py:313-315
+        out[t] = bold(y)
+    return out

@@ -536,6 +536,31 @@ def case_monitors(R):
     save('monitors_40', **out)
 
 
+def case_balloon(R):
+    """BalloonModel (tvb/analyzers/fmri_balloon.py) on a seeded smooth random
+    series (3000 samples at 1 ms, 2 variables, 6 regions, 1 mode) for the
+    non-linear and linear BOLD equations, the classical and revised
+    coefficients, and the none / sum / abs_diff input transformations with
+    and without mean subtraction."""
+    from tvb.datatypes.time_series import TimeSeries
+    from tvb.analyzers.fmri_balloon import BalloonModel, BoldModels, NeuralInputTransformations as NIT
+    rng = np.random.default_rng(5)
+    T, n = 3000, 6
+    x = np.cumsum(rng.normal(size=(T, 2, n, 1)), axis=0) * 0.01 + 0.1
+    out = dict(x=x)
+    cases = {'nl_rbm_none': dict(),
+             'lin_rbm_sum': dict(bold_model=BoldModels.LINEAR, neural_input_transformation=NIT.SUM),
+             'nl_cbm_absdiff': dict(RBM=False, neural_input_transformation=NIT.ABS_DIFF),
+             'nl_rbm_norm': dict(normalize_neural_input=True)}
+    for name, kw in cases.items():
+        ts = TimeSeries(data=x, sample_period=1.0, sample_period_unit='ms', time=np.arange(T) * 1.0)
+        bm = BalloonModel(time_series=ts, **kw)
+        res = bm.evaluate()
+        out[name] = res.data
+        out[name + '_t'] = res.time
+    save('balloon', **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference/tvb_library')
@@ -564,6 +589,7 @@ def main():
         'jr': lambda: case_jr(R),
         'couplings': lambda: case_couplings(R),
         'monitors': lambda: case_monitors(R),
+        'balloon': lambda: case_balloon(R),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only:

@@ -473,3 +473,19 @@ def test_subsample_global_spatial_average_vs_reference(which):
         if which == 'g2d':
             np.testing.assert_allclose(t, fx['g2d_%s_t' % name], rtol=0, atol=1e-12)
         report('%s %s vs reference' % (which, name), y[..., 0], ref, 1e-4)
+
+
+@pytest.mark.parametrize('case', ['nl_rbm_none', 'lin_rbm_sum', 'nl_cbm_absdiff', 'nl_rbm_norm'])
+def test_balloon_device_vs_reference(case):
+    """The float64 Balloon-Windkessel kernel (tvbk_balloon) through the drop-in BalloonModel against the
+    reference analyzer's output, for both BOLD equations, both coefficient sets and the three input
+    transformations."""
+    from tvb_b200.analyzers import BalloonModel
+    fx = G.load('balloon')
+    kw = dict(nl_rbm_none={}, lin_rbm_sum=dict(bold_model='linear', neural_input_transformation='sum'),
+              nl_cbm_absdiff=dict(RBM=False, neural_input_transformation='abs_diff'),
+              nl_rbm_norm=dict(normalize_neural_input=True))[case]
+    res = BalloonModel(fx['x'], sample_period=1.0, sample_period_unit='ms', time=np.arange(3000) * 1.0,
+                       **kw).evaluate()
+    np.testing.assert_allclose(res.time, fx[case + '_t'], rtol=0, atol=1e-12)
+    report('balloon %s vs reference' % case, res.data, fx[case], 1e-10)

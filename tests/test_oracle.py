@@ -243,3 +243,27 @@ def test_subsample_global_spatial_average_monitors():
     for (t, y), name in zip(out, ('sub', 'glob', 'spat', 'tavg')):
         ref = fx['rww_' + name]
         assert np.abs(y - ref).max() / np.abs(ref).max() < 1e-9, name
+
+
+@pytest.mark.parametrize('case', ['nl_rbm_none', 'lin_rbm_sum', 'nl_cbm_absdiff', 'nl_rbm_norm'])
+def test_balloon_oracle_vs_reference(case):
+    """Balloon-Windkessel BOLD (tvb/analyzers/fmri_balloon.py) restated in the oracle vs the reference."""
+    fx = G.load('balloon')
+    x = fx['x']
+    kw = dict(nl_rbm_none=('none', False, True, True), lin_rbm_sum=('sum', False, False, True),
+              nl_cbm_absdiff=('abs_diff', False, True, False), nl_rbm_norm=('none', True, True, True))[case]
+    mode, norm, nonlinear, rbm = kw
+    if mode == 'none':
+        xi = x[:, 0, :, 0]
+    elif mode == 'sum':
+        xi = x.sum(axis=1)[:, :, 0]
+    else:
+        xi = np.abs(np.diff(x, axis=0))[:, 0, :, 0]
+    if norm:
+        xi = xi - xi.mean(axis=0)
+    E0, TE, eps, nu0, r0 = 0.4, 0.04, 0.5, 40.3, 25.0
+    k = (4.3 * nu0 * E0 * TE, eps * r0 * E0 * TE, 1 - eps) if rbm else (7. * E0, 2. * E0, 1. - eps)
+    out = O.balloon_bold(xi, 0.001, k=k, nonlinear=nonlinear)
+    ref = fx[case][:, 0, :, 0]
+    assert out.shape == ref.shape
+    assert np.abs(out - ref).max() / np.abs(ref).max() < 1e-12

@@ -125,6 +125,7 @@ _SIGNATURES = {
     'tvbk_sim_run': (_I32, [ctypes.POINTER(Launch), _P]),
     'tvbk_gather_delayed': (_I32, [ctypes.POINTER(Inst), _I32, _I64, _P, _P]),
     'tvbk_fc': (_I32, [_P, _I32, _I32, _I32, _P, _P]),
+    'tvbk_balloon': (_I32, [_P, _I32, _I64, _D, _P, _I32, _P, _P]),
     'tvbk_sim_run_static': (_I32, [ctypes.POINTER(Launch), ctypes.POINTER(Inst), _P, _P]),
 }
 
