@@ -120,6 +120,11 @@ typedef struct tvbk_inst {
     const float* params;         /* [nparam][n] model parameters, one value per region */
     const float* noise_sigma;    /* [nintvar][n] sqrt(dt) * sqrt(2 nsig); NULL when deterministic */
     const float* noise_fed;      /* [*][nintvar][n] standard normals; step s reads row s - fed_base - 1 */
+    /* region stimulus (patterns.py:146-186, simulator.py:290-306): step s adds
+     * stim[s - stim_base - 1] * stim_weight[i] to the state variables in the
+     * stim_vars bit mask, through dt * stimulus in the scheme (identity: + stimulus) */
+    const float* stim;           /* [*] temporal pattern; NULL: no stimulus */
+    const float* stim_weight;    /* [n] spatial pattern */
     /* monitors (NULL disables one) */
     float* raw;                  /* [*][nvoi][n]; step s writes row s - raw_base - 1 */
     float* sub;                  /* [*][nvoi][n] the state at every step s with s % sub_istep == 0 (SubSample,
@@ -132,9 +137,10 @@ typedef struct tvbk_inst {
     const double* hrf;           /* [stock_len] reversed haemodynamic kernel */
     int64_t step;                /* last completed step (the reference's current_step) */
     int64_t step_end;            /* run until step == step_end */
-    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base;
+    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base, stim_base;
     int32_t n, nnz, horizon, ring_len;
     int32_t tavg_istep, bold_istep, bold_ii, stock_len, sub_istep;
+    uint32_t stim_vars;          /* bit k: state variable k receives the stimulus (the model's stvar) */
     float cfun[6];               /* coupling parameters, see tvbk_sim_run */
     uint32_t seed, stream;       /* Philox key */
     double bold_k1v0;            /* k_1 * V_0 of the FirstOrderVolterra kernel */

@@ -339,14 +339,17 @@ class Monitor:
 
 def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, coupling_params,
              integrator, n_steps, monitors, buffer0, state0, step0=0, nsig=None, noise_z=None,
-             history_dtype=np.float32, voi=None, bounds=None):
+             history_dtype=np.float32, voi=None, bounds=None, stimulus=None):
     """Run the region simulation loop of Simulator.__call__ (tvb/simulator/simulator.py:322-366).
 
     buffer0: (H, ncvar, n) initial history ring as configured by the reference
     (tvb/simulator/history.py:73-158); state0: (nsv, n) float64 current state;
     step0: current_step.  noise_z: (n_steps, nintvar, n) standard normals
-    (the noise of step k is sqrt(dt) * noise_z[k]).  Returns a list, one entry
-    per monitor, of (times, data[T, nvoi, n]).
+    (the noise of step k is sqrt(dt) * noise_z[k]).  stimulus: (temporal,
+    weight, stvar) -- step k of the run adds weight * temporal[k] to the state
+    variables stvar through the scheme's stimulus term (simulator.py:290-306,
+    patterns.py:116-134).  Returns a list, one entry per monitor, of
+    (times, data[T, nvoi, n]).
     """
     info = MODEL_INFO.get(model)
     p = dict(MODEL_DEFAULTS.get(model, {}))
@@ -435,30 +438,36 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
 
     start = step0 + 1
     c = couple(start)
+    stim = 0.0
+    if stimulus is not None:
+        s_temporal, s_weight, s_vars = stimulus
+        stim = np.zeros_like(X)
     for k, step in enumerate(range(start, start + n_steps)):
+        if stimulus is not None:
+            stim[np.asarray(s_vars)] = np.asarray(s_weight, dtype=np.float64) * s_temporal[k]
         if integrator == 'HeunDeterministic':          # integrators.py:296-318
             m0 = dfun(X, c, p)
-            inter = X + dt * (m0 + 0.0)
+            inter = X + dt * (m0 + stim)
             bound(inter)
             dX = (m0 + dfun(inter, c, p)) * dt / 2.0
-            X = X + dX + dt * 0.0
+            X = X + dX + dt * stim
         elif integrator == 'HeunStochastic':           # integrators.py:330-362
             noise = np.sqrt(dt) * noise_z[k]
             m0 = dfun(X, c, p)
             noise = noise * gfun
-            inter = X + dt * m0 + noise + dt * 0.0
+            inter = X + dt * m0 + noise + dt * stim
             bound(inter)
             dX = (m0 + dfun(inter, c, p)) * dt / 2.0
-            X = X + dX + noise + dt * 0.0
+            X = X + dX + noise + dt * stim
         elif integrator == 'EulerDeterministic':       # integrators.py:376-391
             dX = dfun(X, c, p)
-            X = X + dt * (dX + 0.0)
+            X = X + dt * (dX + stim)
         elif integrator == 'EulerStochastic':          # integrators.py:405-426
             noise = np.sqrt(dt) * noise_z[k]
             dX = dfun(X, c, p) * dt
-            X = X + dX + gfun * noise + dt * 0.0
+            X = X + dX + gfun * noise + dt * stim
         elif integrator == 'Identity':                 # integrators.py:494-507
-            X = dfun(X, c, p) + 0.0
+            X = dfun(X, c, p) + stim
         elif integrator == 'RungeKutta4thOrderDeterministic':   # integrators.py:437-480
             dt2, dt6 = dt / 2.0, dt / 6.0
             k1 = dfun(X, c, p)
@@ -471,7 +480,7 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
             i3 = X + dt * k3
             bound(i3)
             k4 = dfun(i3, c, p)
-            X = X + dt6 * (k1 + 2.0 * k2 + 2.0 * k3 + k4) + dt * 0.0
+            X = X + dt6 * (k1 + 2.0 * k2 + 2.0 * k3 + k4) + dt * stim
         else:
             raise NotImplementedError(integrator)
         bound(X)

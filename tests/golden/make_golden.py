@@ -63,10 +63,12 @@ def import_reference(ref):
     import tvb.simulator.noise as noise
     import tvb.simulator.history as history
     from tvb.datatypes.connectivity import Connectivity
+    from tvb.datatypes import equations, patterns
     from tvb.basic.neotraits.api import List
     return dict(simulator=simulator, models=models, coupling=coupling,
                 integrators=integrators, monitors=monitors, noise=noise,
-                history=history, Connectivity=Connectivity, List=List)
+                history=history, Connectivity=Connectivity, List=List,
+                equations=equations, patterns=patterns)
 
 
 FP64_FIELDS = {
@@ -561,6 +563,61 @@ def case_balloon(R):
     save('balloon', **out)
 
 
+def case_stimulus(R):
+    """Region stimuli (StimuliRegion: temporal equation x region weights) on
+    the 40-region connectome of case_couplings: Generic2dOscillator with a
+    PulseTrain (HeunDeterministic, Raw + TemporalAverage 1 ms, 60 ms);
+    Generic2dOscillator with stvar = [1] and a Sinusoid (EulerDeterministic,
+    Raw, 40 ms); ReducedWongWang with an Alpha pulse (EulerStochastic,
+    reference noise, Raw, 40 ms); Epileptor with a Gaussian
+    (RungeKutta4thOrderDeterministic dt 0.05, Raw, 20 ms).  Each case keeps
+    the reference's temporal and spatial patterns."""
+    w, L = synthetic_connectome(40, 0.40, 10.0, 120.0, seed=21)
+    speed = 3.0
+    E, P, M, I, C = R['equations'], R['patterns'], R['models'], R['integrators'], R['coupling']
+    rng = np.random.default_rng(31)
+    weight = np.where(rng.random(40) < 0.5, rng.uniform(0.5, 2.0, 40), 0.0)
+    out = dict(weights=w, tract_lengths=L, speed=speed, stim_weight=weight)
+
+    def g2d_w():
+        m = M.Generic2dOscillator()
+        m.stvar = np.array([1], dtype=np.int32)
+        return m
+    cases = {
+        'g2d_pulse': (M.Generic2dOscillator, C.Linear(a=np.array([0.0152])), lambda: I.HeunDeterministic(dt=0.1),
+                      E.PulseTrain(parameters={'T': 12.0, 'tau': 4.0, 'amp': 2.0, 'onset': 5.0}),
+                      lambda: [R['monitors'].Raw(), R['monitors'].TemporalAverage(period=1.0)], 60.0, 301),
+        'g2d_w_sin': (g2d_w, C.Linear(a=np.array([0.0152])), lambda: I.EulerDeterministic(dt=0.1),
+                      E.Sinusoid(parameters={'amp': 0.5, 'frequency': 0.05}),
+                      lambda: [R['monitors'].Raw()], 40.0, 302),
+        'rww_alpha': (M.ReducedWongWang, C.Linear(a=np.array([0.3])),
+                      lambda: I.EulerStochastic(dt=0.1, noise=R['noise'].Additive(nsig=np.array([1e-4]))),
+                      E.Alpha(parameters={'onset': 3.0, 'alpha': 0.5, 'beta': 1.0}),
+                      lambda: [R['monitors'].Raw()], 40.0, None),
+        'epi_gauss': (M.Epileptor, C.Linear(a=np.array([0.01])), lambda: I.RungeKutta4thOrderDeterministic(dt=0.05),
+                      E.Gaussian(parameters={'amp': 1.5, 'sigma': 4.0, 'midpoint': 10.0, 'offset': 0.0}),
+                      lambda: [R['monitors'].Raw()], 20.0, 303),
+    }
+    for name, (model, cf, integ, eq, mons, length, seed) in cases.items():
+        def build(model=model, cf=cf, integ=integ, eq=eq, mons=mons, length=length):
+            conn = make_conn(R, w, L, speed)
+            stim = P.StimuliRegion(temporal=eq, connectivity=conn, weight=weight)
+            return R['simulator'].Simulator(model=model(), connectivity=conn, coupling=cf, integrator=integ(),
+                                            monitors=mons(), simulation_length=length, stimulus=stim)
+        sim, cfg, res, rec, _ = run_sim(R, build, length, False, ic_seed=seed, record_noise=seed is None)
+        out[name + '_temporal'] = np.asarray(sim.stimulus.temporal_pattern).reshape(-1)
+        out[name + '_spatial'] = np.asarray(sim.stimulus.spatial_pattern).reshape(-1)
+        out[name + '_stvar'] = np.asarray(sim.model.stvar, dtype=np.int32)
+        out[name + '_buffer0'] = cfg['buffer0']
+        out[name + '_state0'] = cfg['state0']
+        for k, (t, y) in enumerate(res):
+            out['%s_m%d' % (name, k)] = y[..., 0]
+            out['%s_m%d_t' % (name, k)] = t
+        if rec is not None:
+            out[name + '_noise_sha256'] = rec.h.hexdigest()
+    save('stimulus_40', **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference/tvb_library')
@@ -590,6 +647,7 @@ def main():
         'couplings': lambda: case_couplings(R),
         'monitors': lambda: case_monitors(R),
         'balloon': lambda: case_balloon(R),
+        'stimulus': lambda: case_stimulus(R),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only:

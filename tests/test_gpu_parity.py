@@ -489,3 +489,107 @@ def test_balloon_device_vs_reference(case):
                        **kw).evaluate()
     np.testing.assert_allclose(res.time, fx[case + '_t'], rtol=0, atol=1e-12)
     report('balloon %s vs reference' % case, res.data, fx[case], 1e-10)
+
+
+STIM_GPU = {
+    'g2d_pulse': ('Generic2dOscillator', None, lambda c: c.Linear(a=0.0152), 'HeunDeterministic', 0.1, 60.0, 301,
+                  'PulseTrain', {'T': 12.0, 'tau': 4.0, 'amp': 2.0, 'onset': 5.0}),
+    'g2d_w_sin': ('Generic2dOscillator', [1], lambda c: c.Linear(a=0.0152), 'EulerDeterministic', 0.1, 40.0, 302,
+                  'Sinusoid', {'amp': 0.5, 'frequency': 0.05}),
+    'rww_alpha': ('ReducedWongWang', None, lambda c: c.Linear(a=0.3), 'EulerStochastic', 0.1, 40.0, None,
+                  'Alpha', {'onset': 3.0, 'alpha': 0.5, 'beta': 1.0}),
+    'epi_gauss': ('Epileptor', None, lambda c: c.Linear(a=0.01), 'RungeKutta4thOrderDeterministic', 0.05, 20.0,
+                  303, 'Gaussian', {'amp': 1.5, 'sigma': 4.0, 'midpoint': 10.0, 'offset': 0.0}),
+}
+
+
+@pytest.mark.parametrize('case', sorted(STIM_GPU))
+def test_region_stimulus_vs_reference(case):
+    """A StimuliRegion (temporal equation x region weights, patterns.py:146-186) added through each scheme's
+    stimulus term (integrators.py:296-480) on the device against the reference's own runs: Heun, Euler, Euler
+    stochastic (the reference's noise stream) and RK4; stvar = cvar and stvar = [1]."""
+    from tvb_b200 import equations
+    from tvb_b200.patterns import StimuliRegion
+    T = tvb()
+    fx = G.load('stimulus_40')
+    model_name, stvar, cf, integ_name, dt, length, seed, eq, params = STIM_GPU[case]
+    model = getattr(T['models'], model_name)()
+    if stvar is not None:
+        model.stvar = np.array(stvar)
+    I = T['integrators']
+    if integ_name == 'EulerStochastic':
+        integ = I.EulerStochastic(dt=dt, noise=T['noise'].Additive(nsig=[1e-4]))
+    else:
+        integ = getattr(I, integ_name)(dt=dt)
+    mons = [T['monitors'].Raw()]
+    if case == 'g2d_pulse':
+        mons.append(T['monitors'].TemporalAverage(period=1.0))
+    conn = T['Connectivity'](weights=fx['weights'], tract_lengths=fx['tract_lengths'], speed=float(fx['speed']))
+    stim = StimuliRegion(temporal=equations.EQUATIONS[eq](params), connectivity=conn, weight=fx['stim_weight'])
+    if seed is not None:
+        np.random.seed(seed)
+    sim = T['Simulator'](model=model, connectivity=conn, coupling=cf(T['coupling']), integrator=integ,
+                         monitors=mons, simulation_length=length, stimulus=stim,
+                         noise_source='reference').configure()
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx[case + '_buffer0'])
+    res = sim.run()
+    # Epileptor driven by the Gaussian pulse amplifies perturbations: a 1e-7 relative change of the initial
+    # state moves the float64 reference trajectory by 1.9e-5 over these 400 RK4 steps, so float32 rounding
+    # at every step ends near 1e-4; its bound is 5e-4 (RMS 1e-4)
+    bound = 5e-4 if case == 'epi_gauss' else 1e-4
+    for k, (t, y) in enumerate(res):
+        np.testing.assert_allclose(t, fx['%s_m%d_t' % (case, k)], rtol=0, atol=1e-12)
+        _, rms = report('stimulus %s m%d vs reference' % (case, k), y[..., 0], fx['%s_m%d' % (case, k)], bound)
+        assert rms <= 1e-4, (case, k, rms)
+
+
+def test_stimulus_weight_sweep_on_every_kernel():
+    """A sweep over stimulus sites ('stimulus.weight', one weight vector per instance) on the row kernel (rings in
+    shared or global memory), instance lanes, the cluster kernel (4 CTAs), the edge-parallel and the split
+    kernels gives the same trajectories, each instance equal to its own Simulator run; the stimulus changes
+    the run."""
+    from tvb_b200 import coupling, equations, integrators, models, monitors, noise, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.patterns import StimuliRegion
+    from tvb_b200.simulator import Simulator
+    from tvb_b200.sweep import ParameterSweep
+    n, I = 68, 8
+    w, L = synthetic.connectome(n, 0.3, 10.0, 200.0, seed=3)
+    rng = np.random.default_rng(2)
+    weights = np.zeros((I, n))
+    for i in range(I):
+        weights[i, rng.choice(n, 4, replace=False)] = rng.uniform(0.05, 0.2, 4)
+    stim = StimuliRegion(temporal=equations.PulseTrain({'T': 50.0, 'tau': 10.0, 'amp': 1.0, 'onset': 20.0}),
+                         weight=weights[0])
+
+    def integ():
+        return integrators.EulerStochastic(dt=0.1, noise=noise.Additive(nsig=[1e-4]))
+    mons, length = [monitors.TemporalAverage(period=1.0)], 400.0
+    out = {}
+    for gather, lanes, smem, cluster in [('row', 1, True, 0), ('row', 1, False, 0), ('row', 'auto', None, 0),
+                                         ('row', 1, False, 4), ('edge', 1, None, 0), ('split', 1, True, 0)]:
+        np.random.seed(11)
+        sw = ParameterSweep(model=models.ReducedWongWang(), connectivity=Connectivity(w, L, speed=5.0),
+                            coupling=coupling.Linear(a=0.2), integrator=integ(), monitors=mons,
+                            simulation_length=length, sweep={'stimulus.weight': weights}, gather=gather,
+                            lanes=lanes, ring_in_smem=smem, cluster=cluster, stimulus=stim).configure()
+        res = sw.run(fc=False)
+        assert (res['status'] == 0).all()
+        out[(gather, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster)] = res['tavg']
+    base = out[('row', 1, True, 0)]
+    for key, tavg in out.items():
+        if key != ('row', 1, True, 0):
+            report('stimulus sweep %s vs row' % (key,), tavg, base, 1e-5)
+    # instance 3 alone through the Simulator (its Philox stream id is the instance index)
+    np.random.seed(11)
+    sim = Simulator(model=models.ReducedWongWang(), connectivity=Connectivity(w, L, speed=5.0),
+                    coupling=coupling.Linear(a=0.2), integrator=integ(), monitors=mons, simulation_length=length,
+                    stimulus=StimuliRegion(temporal=stim.temporal, weight=weights[3]), stream_id=3).configure()
+    (t, y), = sim.run()
+    report('stimulus sweep instance 3 vs Simulator', base[3], y[..., 0], 1e-5)
+    np.random.seed(11)
+    sw = ParameterSweep(model=models.ReducedWongWang(), connectivity=Connectivity(w, L, speed=5.0),
+                        coupling=coupling.Linear(a=0.2), integrator=integ(), monitors=mons,
+                        simulation_length=length, sweep={'coupling.a': np.full(I, 0.2)}).configure()
+    plain = sw.run(fc=False)['tavg']
+    assert rel_err(plain, base)[0] > 1e-3

@@ -267,3 +267,41 @@ def test_balloon_oracle_vs_reference(case):
     ref = fx[case][:, 0, :, 0]
     assert out.shape == ref.shape
     assert np.abs(out - ref).max() / np.abs(ref).max() < 1e-12
+
+
+STIM_CASES = {
+    # case: model, model params, coupling, coupling params, integrator, dt, steps, monitors, nsig
+    'g2d_pulse': ('Generic2dOscillator', 'Linear', {'a': 0.0152}, 'HeunDeterministic', 0.1, 600,
+                  lambda: [O.Monitor('Raw'), O.Monitor('TemporalAverage', 1.0)], None),
+    'g2d_w_sin': ('Generic2dOscillator', 'Linear', {'a': 0.0152}, 'EulerDeterministic', 0.1, 400,
+                  lambda: [O.Monitor('Raw')], None),
+    'rww_alpha': ('ReducedWongWang', 'Linear', {'a': 0.3}, 'EulerStochastic', 0.1, 400,
+                  lambda: [O.Monitor('Raw')], [1e-4]),
+    'epi_gauss': ('Epileptor', 'Linear', {'a': 0.01}, 'RungeKutta4thOrderDeterministic', 0.05, 400,
+                  lambda: [O.Monitor('Raw')], None),
+}
+
+
+@pytest.mark.parametrize('case', sorted(STIM_CASES))
+def test_region_stimulus(case):
+    """StimuliRegion through the scheme's stimulus term (simulator.py:290-306, integrators.py:296-530) against
+    reference runs: PulseTrain / Sinusoid / Alpha / Gaussian temporal patterns, stvar = cvar and stvar = [1]."""
+    fx = G.load('stimulus_40')
+    model, cf, cp, integ, dt, n_steps, mons, nsig = STIM_CASES[case]
+    z = None
+    if nsig is not None:
+        H = fx[case + '_buffer0'].shape[0]
+        z = O.reference_noise(42, [O.MODEL_INFO[model]['ranges']['S']], H, 40, 1, n_steps)
+    stim = (fx[case + '_temporal'], fx[case + '_spatial'], fx[case + '_stvar'])
+    out, _ = O.simulate(model, {}, fx['weights'], fx['tract_lengths'], float(fx['speed']), dt, cf, cp, integ, n_steps,
+                        mons(), fx[case + '_buffer0'], fx[case + '_state0'], 0, nsig=nsig, noise_z=z, stimulus=stim)
+    for k, (t, y) in enumerate(out):
+        ref = fx['%s_m%d' % (case, k)]
+        np.testing.assert_allclose(t, fx['%s_m%d_t' % (case, k)], rtol=0, atol=1e-12)
+        err = np.abs(y - ref).max() / np.abs(ref).max()
+        assert err < 1e-9, (case, k, err)
+    # the stimulus changes the run: without it the oracle departs from the reference
+    out0, _ = O.simulate(model, {}, fx['weights'], fx['tract_lengths'], float(fx['speed']), dt, cf, cp, integ,
+                         n_steps, mons(), fx[case + '_buffer0'], fx[case + '_state0'], 0, nsig=nsig, noise_z=z)
+    ref = fx['%s_m0' % case]
+    assert np.abs(out0[0][1] - ref).max() / np.abs(ref).max() > 1e-4

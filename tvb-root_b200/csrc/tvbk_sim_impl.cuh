@@ -273,6 +273,9 @@ struct Node {
     double bacc[MV];
     float* raw_p;
     const float* fed_p;
+    const float* stim_p;  // temporal stimulus of the launch's first step (NULL: none)
+    float stim_w;         // this region's spatial weight
+    uint32_t stim_vars;
     float* tavg_p;
     double* bold_p;
     float* sub_p;
@@ -323,6 +326,9 @@ struct Node {
         sub_p = Ip->sub ? Ip->sub + (size_t)(s0 / Ip->sub_istep - Ip->sub_base) * nvoi * n + i : nullptr;
         raw_p = Ip->raw ? Ip->raw + (size_t)(s0 - Ip->raw_base) * nvoi * n + i : nullptr;
         fed_p = Ip->noise_fed ? Ip->noise_fed + (size_t)(s0 - Ip->fed_base) * NINT * n + i : nullptr;
+        stim_p = Ip->stim ? Ip->stim + (s0 - Ip->stim_base) : nullptr;
+        stim_w = Ip->stim ? Ip->stim_weight[i] : 0.0f;
+        stim_vars = Ip->stim ? Ip->stim_vars : 0u;
         tavg_p = do_tavg ? Ip->tavg + (size_t)(s0 / Ip->tavg_istep - Ip->tavg_base) * nvoi * n + i : nullptr;
         bold_p = do_bold ? Ip->bold + (size_t)(s0 / Ip->bold_istep - Ip->bold_base) * nvoi * n + i : nullptr;
     }
@@ -338,30 +344,42 @@ struct Node {
         }
     }
 
-    // The scheme step with coupling input c and standard normals z (integrators.py:296-426),
-    // then the state-variable bounds.
-    __device__ __forceinline__ void integrate(const float* c, const float* z, float dt) {
-        float m0[NSV];
+    // Stimulus of step s0 + 1 + ks: spatial weight x temporal pattern (patterns.py:116-134).
+    __device__ __forceinline__ float stim_at(int ks) const {
+        return stim_p != nullptr ? stim_w * __ldg(stim_p + ks) : 0.0f;
+    }
+
+    // The scheme step with coupling input c, standard normals z and stimulus
+    // value st (integrators.py:296-530), then the state-variable bounds.  The
+    // stimulus reaches the variables in stim_vars; with none the added terms
+    // are exact zeros and the step is the unstimulated one bit for bit.
+    __device__ __forceinline__ void integrate(const float* c, const float* z, float dt, float st) {
+        float m0[NSV], sv[NSV];
         M::dfun(x, c, p, m0);
+#pragma unroll
+        for (int k = 0; k < NSV; ++k) sv[k] = ((stim_vars >> k) & 1u) ? st : 0.0f;
         if constexpr (SCHEME == TVBK_SCHEME_EULER_DET) {
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k];
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * (m0[k] + sv[k]);
         } else if constexpr (SCHEME == TVBK_SCHEME_EULER_STOCH) {
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k] + sig[k] * z[k];
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k] + sig[k] * z[k] + dt * sv[k];
         } else if constexpr (SCHEME == TVBK_SCHEME_HEUN_DET || SCHEME == TVBK_SCHEME_HEUN_STOCH) {
             float inter[NSV], nz[NSV];
 #pragma unroll
             for (int k = 0; k < NSV; ++k) {
                 nz[k] = STOCH ? sig[k] * z[k] : 0.0f;
-                inter[k] = x[k] + dt * m0[k] + nz[k];
+                if constexpr (STOCH)
+                    inter[k] = x[k] + dt * m0[k] + nz[k] + dt * sv[k];
+                else
+                    inter[k] = x[k] + dt * (m0[k] + sv[k]);
             }
             M::bound(inter);
             float m1[NSV];
             M::dfun(inter, c, p, m1);
             const float hdt = dt * 0.5f;
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + (m0[k] + m1[k]) * hdt + nz[k];
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + (m0[k] + m1[k]) * hdt + nz[k] + dt * sv[k];
         } else if constexpr (SCHEME == TVBK_SCHEME_RK4) {
             const float dt2 = dt * 0.5f, dt6 = dt / 6.0f;
             float st[NSV], k2[NSV], k3[NSV], k4[NSV];
@@ -378,10 +396,11 @@ struct Node {
             M::bound(st);
             M::dfun(st, c, p, k4);
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt6 * (m0[k] + 2.0f * k2[k] + 2.0f * k3[k] + k4[k]);
+            for (int k = 0; k < NSV; ++k)
+                x[k] = x[k] + dt6 * (m0[k] + 2.0f * k2[k] + 2.0f * k3[k] + k4[k]) + dt * sv[k];
         } else {  // identity
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = m0[k];
+            for (int k = 0; k < NSV; ++k) x[k] = m0[k] + sv[k];
         }
         M::bound(x);
     }
@@ -406,7 +425,7 @@ struct Node {
             }
         }
 
-        integrate(c, z, dt);
+        integrate(c, z, dt, stim_at(ks));
 
         // monitors
         if (raw_p != nullptr) {
@@ -765,7 +784,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                         if (r == 1) node.philox_block(i, s + 4, zn);  // the next block's normals
 #pragma unroll
                         for (int k = 0; k < M::NINT; ++k) z[k] = node.zc[k][r];
-                        node.integrate(c, z, L.dt);
+                        node.integrate(c, z, L.dt, node.stim_at(ks + r));
                         node.accumulate(L, n);
                         write(wslot);
                     }
@@ -794,7 +813,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                     // coupling of step s + 1: times s - d with d >= d_min >= 1
                     row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
                     node.fetch_z(L, n, s, z);
-                    node.integrate(c, z, L.dt);
+                    node.integrate(c, z, L.dt, node.stim_at(ks));
                     node.accumulate(L, n);
                     write(wslot);
                 }

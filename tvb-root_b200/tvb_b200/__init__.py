@@ -9,7 +9,7 @@ kernels of libtvbk.so (include/tvbk.h):
     from tvb_b200.sweep import ParameterSweep
 """
 from . import _lib  # noqa: F401  (fails loudly when libtvbk.so is missing)
-from . import coupling, integrators, models, monitors, noise  # noqa: F401
+from . import coupling, equations, integrators, models, monitors, noise, patterns  # noqa: F401
 from .connectivity import Connectivity  # noqa: F401
 
 __version__ = '0.1.0'

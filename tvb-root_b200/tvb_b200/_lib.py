@@ -47,6 +47,8 @@ class Inst(ctypes.Structure):
         ('params', ctypes.c_void_p),
         ('noise_sigma', ctypes.c_void_p),
         ('noise_fed', ctypes.c_void_p),
+        ('stim', ctypes.c_void_p),
+        ('stim_weight', ctypes.c_void_p),
         ('raw', ctypes.c_void_p),
         ('sub', ctypes.c_void_p),
         ('tavg', ctypes.c_void_p),
@@ -62,6 +64,7 @@ class Inst(ctypes.Structure):
         ('tavg_base', ctypes.c_int64),
         ('bold_base', ctypes.c_int64),
         ('sub_base', ctypes.c_int64),
+        ('stim_base', ctypes.c_int64),
         ('n', ctypes.c_int32),
         ('nnz', ctypes.c_int32),
         ('horizon', ctypes.c_int32),
@@ -71,6 +74,7 @@ class Inst(ctypes.Structure):
         ('bold_ii', ctypes.c_int32),
         ('stock_len', ctypes.c_int32),
         ('sub_istep', ctypes.c_int32),
+        ('stim_vars', ctypes.c_uint32),
         ('cfun', ctypes.c_float * 6),
         ('seed', ctypes.c_uint32),
         ('stream', ctypes.c_uint32),

@@ -90,10 +90,13 @@ class InstanceSpec:
     sigma: (nintvar, n) sqrt(dt) sqrt(2 nsig) or None; n_steps: steps to run;
     raw: keep every step; tavg_istep / bold (dict istep, ii, hrf, k1v0): monitors.
     noise_fed: (n_steps, nintvar, n) standard normals or None.
+    stim: region stimulus or None: dict with 'temporal' (the pattern of steps
+    step0 + 1 ..., at least n_steps values), 'weight' (n,) spatial pattern and
+    'vars' (indices of the state variables it drives, the model's stvar).
     """
 
     def __init__(self, conn, ring0, state0, params, cfun, n_steps, step0=0, sigma=None, noise_fed=None,
-                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0):
+                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0, stim=None):
         self.conn = conn
         self.ring0 = ring0
         self.state0 = state0
@@ -109,6 +112,18 @@ class InstanceSpec:
         self.tavg_istep = int(tavg_istep)
         self.bold = bold
         self.sub_istep = int(sub_istep)  # SubSample / GlobalAverage / SpatialAverage period in steps (0: none)
+        if stim is not None:
+            t = np.asarray(stim['temporal'], dtype=np.float32).reshape(-1)
+            if t.size < self.n_steps:
+                raise IndexError('stimulus temporal pattern has %d samples for %d steps' % (t.size, self.n_steps))
+            w = np.asarray(stim['weight'], dtype=np.float32).reshape(-1)
+            if w.size != conn.n:
+                raise ValueError('stimulus weight has %d values for %d regions' % (w.size, conn.n))
+            mask = 0
+            for v in np.asarray(stim['vars'], dtype=np.int64).reshape(-1):
+                mask |= 1 << int(v)
+            stim = dict(temporal=np.ascontiguousarray(t[:self.n_steps]), weight=np.ascontiguousarray(w), mask=mask)
+        self.stim = stim
         # monitor accumulators carried over from a previous run of the same
         # simulation: dict with 'tavg_acc' (nvoi, n), 'bold_acc' (nvoi, n),
         # 'bold_stock' (stock_len, nvoi, n); None starts them at zero
@@ -327,6 +342,9 @@ class Batch:
                 zero.add(('pre_ring', k), RL * n * 4)
             init.add(('state', k), self.nsv * n * 4)
             init.add(('params', k), max(self.nparam, 1) * n * 4)
+            if s.stim is not None:
+                init.add(('stim', k), max(s.n_steps, 1) * 4)
+                init.add(('stim_w', k), n * 4)
             if s.sigma is not None:
                 init.add(('sigma', k), self.nint * n * 4)
             acc_arena = init if s.acc0 is not None else zero
@@ -422,6 +440,13 @@ class Batch:
                 fed = fed.to(dev, dtype=torch.float32).contiguous()
                 self._fed.append(fed)
                 d['noise_fed'] = fed.data_ptr()
+            if s.stim is not None:
+                if s.stim['mask'] >> self.nsv:
+                    raise ValueError('stimulus drives a state variable the model does not have')
+                d['stim'] = put(('stim', k), s.stim['temporal'])
+                d['stim_weight'] = put(('stim_w', k), s.stim['weight'])
+                d['stim_vars'] = s.stim['mask']
+                d['stim_base'] = s.step0
             if s.acc0 is not None:
                 for key, dtype in (('tavg_acc', np.float32), ('bold_acc', np.float64), ('bold_stock', np.float64)):
                     if (key, k) in init.regions and s.acc0.get(key) is not None:

@@ -14,6 +14,7 @@ class Model(HasParams):
     """Base of the device models (tvb/simulator/models/base.py:39-262)."""
     state_variables = ()
     cvar = None
+    stvar = None  # state variables a stimulus drives; None: the coupling variables (models/base.py:91-92)
     state_variable_range = {}
     state_variable_boundaries = None
     variables_of_interest = ()
@@ -35,6 +36,8 @@ class Model(HasParams):
             if name not in self.observable_choices:
                 raise ValueError('%s is not an observable of %s (choices %s)'
                                  % (name, type(self).__name__, self.observable_choices))
+        if self.stvar is None:
+            self.stvar = np.array(self.cvar, dtype=np.int32).copy()
         return self
 
     def initial(self, dt, history_shape, rng=np.random):

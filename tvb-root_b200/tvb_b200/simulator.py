@@ -46,6 +46,8 @@ def adopt_model(model):
     kw = {p: np.asarray(getattr(model, p)) for p in cls._defaults if hasattr(model, p)}
     m = cls(**kw)
     m.variables_of_interest = tuple(getattr(model, 'variables_of_interest', cls.variables_of_interest))
+    if getattr(model, 'stvar', None) is not None:
+        m.stvar = np.asarray(model.stvar, dtype=np.int32).copy()
     return m
 
 
@@ -131,8 +133,6 @@ class Simulator:
                  stimulus=None, noise_source='philox', chunk_steps=200000, device=None, stream_id=0):
         if surface is not None:
             raise NotImplementedError('surface simulations are not supported on the device path')
-        if stimulus is not None:
-            raise NotImplementedError('stimuli are not supported on the device path')
         if noise_source not in ('philox', 'reference'):
             raise ValueError("noise_source must be 'philox' or 'reference'")
         self.connectivity = connectivity
@@ -143,6 +143,7 @@ class Simulator:
         self.simulation_length = float(simulation_length)
         self.initial_conditions = initial_conditions
         self.conduction_speed = conduction_speed
+        self.stimulus = stimulus
         self.noise_source = noise_source
         self.chunk_steps = int(chunk_steps)
         self.device = device
@@ -197,8 +198,45 @@ class Simulator:
         if self.integrator.stochastic:
             self._sigma = noise_sigma(self.integrator.noise.nsig, self.nint, self.number_of_nodes, dt)
         self._acc = None
+        self._stim = None
+        if self.stimulus is not None:
+            if type(self.stimulus).__name__ != 'StimuliRegion':
+                raise NotImplementedError('stimulus %s has no device implementation' % type(self.stimulus).__name__)
+            if hasattr(self.stimulus, 'configure'):
+                self.stimulus.configure()
+            self.stimulus.configure_space()
+            stvar = np.asarray(self.model.stvar, dtype=np.int64).reshape(-1)
+            if stvar.size == 0 or stvar.min() < 0 or stvar.max() >= self.nsv:
+                raise ValueError('model.stvar %s out of range' % stvar.tolist())
         self._configured = True
         return self
+
+    # ------------------------------------------------------------ stimulus
+    def _prepare_stimulus(self):
+        """Temporal pattern on the grid r_[0 : simulation_length : dt], indexed
+        from the step after the current one (simulator.py:290-306): the step
+        s of this run reads index s - (current_step + 1)."""
+        if self.stimulus is None:
+            self._stim = None
+            return
+        time = np.r_[0.0:self.simulation_length:self.integrator.dt]
+        self.stimulus.configure_time(time.reshape((1, -1)))
+        self._stim = dict(temporal=np.asarray(self.stimulus.temporal_pattern, dtype=np.float64).reshape(-1),
+                          weight=np.asarray(self.stimulus.spatial_pattern, dtype=np.float64).reshape(-1),
+                          step0=self.current_step)
+
+    def stimulus_spec(self, n_steps):
+        """The stimulus of steps current_step + 1 .. + n_steps for InstanceSpec (None without one)."""
+        if self.stimulus is None:
+            return None
+        if self._stim is None:
+            self._prepare_stimulus()
+        st = self._stim
+        k0 = self.current_step - st['step0']
+        if k0 + n_steps > st['temporal'].size:
+            raise IndexError('index %d is out of bounds for the stimulus temporal pattern of size %d'
+                             % (k0 + n_steps - 1, st['temporal'].size))
+        return dict(temporal=st['temporal'][k0:k0 + n_steps], weight=st['weight'], vars=self.model.stvar)
 
     def _configure_history(self):
         """Initial history as SparseHistory.from_simulator (tvb/simulator/history.py:73-158)."""
@@ -262,7 +300,7 @@ class Simulator:
                             self.coupling.kernel_params(), n_steps, step0=self.current_step, sigma=self._sigma,
                             noise_fed=fed, seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                             stream=self.stream_id if stream is None else stream, raw=raw, tavg_istep=tavg_istep,
-                            bold=bspec, sub_istep=self._sub_istep)
+                            bold=bspec, sub_istep=self._sub_istep, stim=self.stimulus_spec(n_steps))
         if self._acc is not None:
             spec.acc0 = self._acc
         return spec, noise_kind
@@ -318,6 +356,7 @@ class Simulator:
             n_steps = int(math.ceil(self.simulation_length / self.integrator.dt))
         elif not np.issubdtype(type(n_steps), np.integer):
             raise TypeError('Incorrect type for n_steps: %s, expected integer' % type(n_steps))
+        self._prepare_stimulus()
         left = int(n_steps)
         while left > 0:
             k = min(left, self.chunk_steps)

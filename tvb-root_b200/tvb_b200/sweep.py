@@ -26,7 +26,9 @@ class ParameterSweep:
     sweep: dict mapping 'coupling.<name>', 'noise.nsig', 'model.<name>' or
     'simulation_length' to arrays of one value per instance (for
     'model.<name>' also an (instances, regions) array: one value per region,
-    like the reference's spatialised parameters); 'simulation_length' gives
+    like the reference's spatialised parameters; 'stimulus.weight' takes an
+    (instances, regions) array of stimulus weights, with `stimulus` given);
+    'simulation_length' gives
     instances of uneven lengths, which run in the same launch and retire at
     their own last step.  Noise: 'philox' draws an independent
     device stream per instance (key = (noise_seed, instance index));
@@ -37,8 +39,9 @@ class ParameterSweep:
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
                  noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
-                 gather='auto', lanes=1, cluster='auto'):
+                 gather='auto', lanes=1, cluster='auto', stimulus=None):
         self.model = adopt_model(model)
+        self.stimulus = stimulus
         self.connectivity = adopt_connectivity(connectivity)
         self.coupling = adopt_coupling(coupling)
         self.integrator = adopt_integrator(integrator)
@@ -64,8 +67,10 @@ class ParameterSweep:
         self._sim = Simulator(model=self.model, connectivity=self.connectivity, coupling=self.coupling,
                               integrator=self.integrator, monitors=self.monitors,
                               simulation_length=self.simulation_length, noise_source=self.noise_source,
-                              device=self.device).configure()
+                              device=self.device, stimulus=self.stimulus).configure()
         sim = self._sim
+        if 'stimulus.weight' in self.sweep and self.stimulus is None:
+            raise ValueError("sweeping 'stimulus.weight' needs a stimulus")
         self.n_steps = int(np.ceil(self.simulation_length / self.integrator.dt))
         n = sim.number_of_nodes
         conn = sim._conn
@@ -85,10 +90,18 @@ class ParameterSweep:
             self.n_steps = int(self.n_steps_each.max())
         else:
             self.n_steps_each = np.full(self.n_instances, self.n_steps, dtype=np.int64)
+        stim = None
+        if self.stimulus is not None:
+            # one time grid covers every instance: r_[0 : L : dt] agrees on the common steps for any L
+            sim.simulation_length = max(self.simulation_length, float(self.n_steps) * self.integrator.dt)
+            sim._prepare_stimulus()
+            stim = sim.stimulus_spec(self.n_steps)
+            sim.simulation_length = self.simulation_length
         for i in range(self.n_instances):
             params = base_params
             cf = self.coupling.kernel_params()
             sigma = sim._sigma
+            stim_i = stim
             for key, vals in self.sweep.items():
                 part, _, name = key.partition('.')
                 if part == 'model':
@@ -102,12 +115,15 @@ class ParameterSweep:
                     sigma = noise_sigma(np.array([vals[i]]), sim.nint, n, self.integrator.dt)
                 elif key == 'simulation_length':
                     pass
+                elif key == 'stimulus.weight':
+                    stim_i = dict(stim, weight=np.asarray(vals[i], dtype=np.float64).reshape(-1))
                 else:
                     raise ValueError('cannot sweep %s' % key)
             spec = InstanceSpec(conn, sim.history_buffer[..., 0], sim.current_state[..., 0], params, cf,
                                 int(self.n_steps_each[i]), step0=sim.current_step, sigma=sigma, noise_fed=None,
                                 seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
-                                stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep)
+                                stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep,
+                                stim=stim_i)
             specs.append(spec)
         self._specs = specs
         noise_kind = _lib.NOISE_NONE
