@@ -51,6 +51,8 @@ extern "C" {
 /* per-instance status bits written by the simulation kernel */
 #define TVBK_STATUS_NONFINITE 1   /* a state variable became NaN or Inf */
 #define TVBK_STATUS_DEGREE 2      /* a row had more edges than launch.max_degree (coupling incomplete) */
+#define TVBK_STATUS_UNSUPPORTED 4 /* the instance asks for an output this kernel variant does not write
+                                   * (AfferentCoupling on a variant other than the row kernel) */
 
 /* components */
 enum {
@@ -130,6 +132,10 @@ typedef struct tvbk_inst {
     float* sub;                  /* [*][nvoi][n] the state at every step s with s % sub_istep == 0 (SubSample,
                                   * and GlobalAverage / SpatialAverage reduce it): row s / sub_istep - sub_base - 1 */
     float* tavg;                 /* [*][nvoi][n]; sample s / tavg_istep - tavg_base - 1 */
+    float* aff;                  /* [*][ncvar][n] AfferentCoupling (monitors.py:394-433): the coupling that step
+                                  * s + 1 receives, taken after step s and averaged over aff_istep steps (1: every
+                                  * step); sample s / aff_istep - aff_base - 1.  Row kernel only */
+    float* aff_acc;              /* [ncvar][n] running sum of the current aff_istep period */
     float* tavg_acc;             /* [nvoi][n] running sum of the current period */
     double* bold;                /* [*][nvoi][n]; sample s / bold_istep - bold_base - 1 */
     double* bold_acc;            /* [nvoi][n] running sum of the current 4 ms window */
@@ -137,10 +143,11 @@ typedef struct tvbk_inst {
     const double* hrf;           /* [stock_len] reversed haemodynamic kernel */
     int64_t step;                /* last completed step (the reference's current_step) */
     int64_t step_end;            /* run until step == step_end */
-    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base, stim_base;
+    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base, stim_base, aff_base;
     int32_t n, nnz, horizon, ring_len;
     int32_t tavg_istep, bold_istep, bold_ii, stock_len, sub_istep;
     uint32_t stim_vars;          /* bit k: state variable k receives the stimulus (the model's stvar) */
+    int32_t aff_istep;
     float cfun[6];               /* coupling parameters, see tvbk_sim_run */
     uint32_t seed, stream;       /* Philox key */
     double bold_k1v0;            /* k_1 * V_0 of the FirstOrderVolterra kernel */
@@ -182,6 +189,10 @@ typedef struct tvbk_launch {
                                   * place (lanes 1, row gather, rings not in shared memory) */
     int32_t cluster_edges;       /* cluster kernel: edges of one CTA's rows that it stages in shared memory; a CTA
                                   * with more edges reads them from global memory (0: always global) */
+    int32_t extras;              /* bit 0: some instance has a region stimulus; bit 1: some instance has an
+                                  * AfferentCoupling monitor.  0 lets the row kernel with rings in shared memory
+                                  * use a build without either (an instance that has one then gets
+                                  * TVBK_STATUS_UNSUPPORTED) */
     int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */
     float dt;
 } tvbk_launch;

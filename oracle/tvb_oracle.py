@@ -411,13 +411,17 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
     # monitors
     hrf, stock_steps = bold_hrf()
     mstate = []
+    afferent_rows = 1 if coupling == 'SigmoidalJansenRit' else len(cvar)
     for m in monitors:
         st = dict(m=m)
-        mv = list(range(len(voi))) if m.voi is None else list(m.voi)
+        if m.kind.startswith('AfferentCoupling'):                 # monitors.py:406-409: coupling rows
+            mv = list(range(afferent_rows)) if m.voi is None else list(m.voi)
+        else:
+            mv = list(range(len(voi))) if m.voi is None else list(m.voi)
         st['voi'] = mv
-        if m.kind == 'Raw':
+        if m.kind in ('Raw', 'AfferentCoupling'):
             st['istep'] = 1
-        elif m.kind == 'TemporalAverage':
+        elif m.kind in ('TemporalAverage', 'AfferentCouplingTemporalAverage'):
             st['istep'] = iround(m.period / dt)
             st['stock'] = np.zeros((st['istep'], len(mv), X.shape[1]))
         elif m.kind in ('SubSample', 'GlobalAverage', 'SpatialAverage'):
@@ -489,11 +493,12 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
         obs = observe(model, X, voi) if info else X      # simulator.py:314-320
         for st in mstate:
             m = st['m']
-            o = obs[st['voi']]
-            if m.kind == 'Raw':                          # monitors.py:188-190
+            # AfferentCoupling monitors see node_coupling of step + 1 (simulator.py:314-320)
+            o = (c if m.kind.startswith('AfferentCoupling') else obs)[st['voi']]
+            if m.kind in ('Raw', 'AfferentCoupling'):    # monitors.py:188-190,411-412
                 st['t'].append(step * dt)
                 st['y'].append(o.copy())
-            elif m.kind == 'TemporalAverage':            # monitors.py:380-391
+            elif m.kind in ('TemporalAverage', 'AfferentCouplingTemporalAverage'):   # monitors.py:380-391
                 st['stock'][(step % st['istep']) - 1] = o
                 if step % st['istep'] == 0:
                     st['t'].append((step - st['istep'] / 2.0) * dt)

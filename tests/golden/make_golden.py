@@ -618,6 +618,43 @@ def case_stimulus(R):
     save('stimulus_40', **out)
 
 
+def case_afferent(R):
+    """AfferentCoupling and AfferentCouplingTemporalAverage (the coupling each
+    step receives next) on the 40-region connectome of case_couplings:
+    Generic2dOscillator with Linear a=0.0152 (HeunDeterministic dt 0.1, 40 ms,
+    both monitors and Raw); Epileptor with Difference a=0.1 (two coupling
+    variables, HeunDeterministic dt 0.05, 20 ms, AfferentCoupling and the
+    period-1 ms average of coupling variable 1); JansenRit with
+    SigmoidalJansenRit (one coupling row, HeunDeterministic dt 0.1, 40 ms)."""
+    w, L = synthetic_connectome(40, 0.40, 10.0, 120.0, seed=21)
+    speed = 3.0
+    M, I, C = R['models'], R['integrators'], R['coupling']
+    Mo = R['monitors']
+    out = dict(weights=w, tract_lengths=L, speed=speed)
+    cases = {
+        'g2d': (M.Generic2dOscillator, lambda: C.Linear(a=np.array([0.0152])), 0.1, 40.0, 401,
+                lambda: [Mo.AfferentCoupling(), Mo.AfferentCouplingTemporalAverage(period=1.0), Mo.Raw()]),
+        'epi': (M.Epileptor, lambda: C.Difference(a=np.array([0.1])), 0.05, 20.0, 402,
+                lambda: [Mo.AfferentCoupling(),
+                         Mo.AfferentCouplingTemporalAverage(period=1.0, variables_of_interest=np.array([1]))]),
+        'jr': (M.JansenRit, lambda: C.SigmoidalJansenRit(a=np.array([10.0])), 0.1, 40.0, 403,
+               lambda: [Mo.AfferentCoupling(variables_of_interest=np.array([0])),
+                        Mo.AfferentCouplingTemporalAverage(period=2.0, variables_of_interest=np.array([0]))]),
+    }
+    for name, (model, cf, dt, length, seed, mons) in cases.items():
+        def build(model=model, cf=cf, dt=dt, mons=mons, length=length):
+            return R['simulator'].Simulator(model=model(), connectivity=make_conn(R, w, L, speed), coupling=cf(),
+                                            integrator=I.HeunDeterministic(dt=dt), monitors=mons(),
+                                            simulation_length=length)
+        sim, cfg, res, _, _ = run_sim(R, build, length, False, ic_seed=seed)
+        out[name + '_buffer0'] = cfg['buffer0']
+        out[name + '_state0'] = cfg['state0']
+        for k, (t, y) in enumerate(res):
+            out['%s_m%d' % (name, k)] = y[..., 0]
+            out['%s_m%d_t' % (name, k)] = t
+    save('afferent_40', **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference/tvb_library')
@@ -648,6 +685,7 @@ def main():
         'monitors': lambda: case_monitors(R),
         'balloon': lambda: case_balloon(R),
         'stimulus': lambda: case_stimulus(R),
+        'afferent': lambda: case_afferent(R),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only:

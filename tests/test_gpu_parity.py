@@ -593,3 +593,70 @@ def test_stimulus_weight_sweep_on_every_kernel():
                         simulation_length=length, sweep={'coupling.a': np.full(I, 0.2)}).configure()
     plain = sw.run(fc=False)['tavg']
     assert rel_err(plain, base)[0] > 1e-3
+
+
+AFF_GPU = {
+    'g2d': ('Generic2dOscillator', lambda c: c.Linear(a=0.0152), 0.1, 40.0, 401,
+            lambda M: [M.AfferentCoupling(), M.AfferentCouplingTemporalAverage(period=1.0), M.Raw()]),
+    'epi': ('Epileptor', lambda c: c.Difference(a=0.1), 0.05, 20.0, 402,
+            lambda M: [M.AfferentCoupling(), M.AfferentCouplingTemporalAverage(period=1.0, variables_of_interest=[1])]),
+    'jr': ('JansenRit', lambda c: c.SigmoidalJansenRit(a=10.0), 0.1, 40.0, 403,
+           lambda M: [M.AfferentCoupling(variables_of_interest=[0]),
+                      M.AfferentCouplingTemporalAverage(period=2.0, variables_of_interest=[0])]),
+}
+
+
+@pytest.mark.parametrize('case', sorted(AFF_GPU))
+def test_afferent_coupling_vs_reference(case):
+    """AfferentCoupling and AfferentCouplingTemporalAverage on the device (the row kernel's prefetched gather
+    for Linear and SigmoidalJansenRit, an extra gather after the barrier for Difference) against the
+    reference's runs; a run split in three launches continues the period average."""
+    T = tvb()
+    fx = G.load('afferent_40')
+    model, cf, dt, length, seed, mons = AFF_GPU[case]
+    conn = T['Connectivity'](weights=fx['weights'], tract_lengths=fx['tract_lengths'], speed=float(fx['speed']))
+
+    def make(chunk):
+        np.random.seed(seed)
+        return T['Simulator'](model=getattr(T['models'], model)(), connectivity=conn, coupling=cf(T['coupling']),
+                              integrator=T['integrators'].HeunDeterministic(dt=dt), monitors=mons(T['monitors']),
+                              simulation_length=length, chunk_steps=chunk).configure()
+    sim = make(200000)
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx[case + '_buffer0'])
+    res = sim.run()
+    for k, (t, y) in enumerate(res):
+        np.testing.assert_allclose(t, fx['%s_m%d_t' % (case, k)], rtol=0, atol=1e-12)
+        report('afferent %s m%d vs reference' % (case, k), y[..., 0], fx['%s_m%d' % (case, k)], 1e-4)
+    # chunks of 137 steps: the period sums carry over between launches
+    res2 = make(137).run()
+    for (t, y), (t2, y2) in zip(res, res2):
+        np.testing.assert_array_equal(t, t2)
+        np.testing.assert_array_equal(y, y2)
+    # the period average alone is taken on the device (above, beside the every-step monitor, it is reduced on
+    # the host from the every-step stream): the same float32 arithmetic, the same bits
+    for chunk in (200000, 137):
+        np.random.seed(seed)
+        only = T['Simulator'](model=getattr(T['models'], model)(), connectivity=conn, coupling=cf(T['coupling']),
+                              integrator=T['integrators'].HeunDeterministic(dt=dt),
+                              monitors=[mons(T['monitors'])[1]], simulation_length=length,
+                              chunk_steps=chunk).configure()
+        assert only._aff_istep == only.monitors[0].istep > 1
+        (t1, y1), = only.run()
+        np.testing.assert_array_equal(t1, res[1][0])
+        np.testing.assert_array_equal(y1, res[1][1])
+
+
+def test_afferent_coupling_stays_on_the_row_kernel():
+    from tvb_b200 import coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.sweep import ParameterSweep
+    w, L = synthetic.connectome(68, 0.3, 10.0, 200.0, seed=3)
+    kw = dict(model=models.ReducedWongWang(), connectivity=Connectivity(w, L, speed=5.0), coupling=coupling.Linear(),
+              integrator=integrators.HeunDeterministic(dt=0.1), monitors=[monitors.AfferentCouplingTemporalAverage(
+                  period=1.0)], simulation_length=20.0, sweep={'coupling.a': np.linspace(0.1, 0.3, 4)})
+    for bad in (dict(cluster=4), dict(gather='split'), dict(gather='edge'), dict(lanes=8)):
+        with pytest.raises(ValueError):
+            ParameterSweep(**kw, **bad).configure().build()
+    res = ParameterSweep(**kw, lanes='auto', cluster='auto').configure().run(fc=False)
+    assert (res['status'] == 0).all()
+    assert res['aff'].shape == (4, 20, 1, 68)

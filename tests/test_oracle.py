@@ -305,3 +305,32 @@ def test_region_stimulus(case):
                          n_steps, mons(), fx[case + '_buffer0'], fx[case + '_state0'], 0, nsig=nsig, noise_z=z)
     ref = fx['%s_m0' % case]
     assert np.abs(out0[0][1] - ref).max() / np.abs(ref).max() > 1e-4
+
+
+AFF_CASES = {
+    'g2d': ('Generic2dOscillator', 'Linear', {'a': 0.0152}, 0.1, 400,
+            lambda: [O.Monitor('AfferentCoupling'), O.Monitor('AfferentCouplingTemporalAverage', 1.0),
+                     O.Monitor('Raw')]),
+    'epi': ('Epileptor', 'Difference', {'a': 0.1}, 0.05, 400,
+            lambda: [O.Monitor('AfferentCoupling'), O.Monitor('AfferentCouplingTemporalAverage', 1.0, voi=[1])]),
+    'jr': ('JansenRit', 'SigmoidalJansenRit', {'a': 10.0}, 0.1, 400,
+           lambda: [O.Monitor('AfferentCoupling', voi=[0]),
+                    O.Monitor('AfferentCouplingTemporalAverage', 2.0, voi=[0])]),
+}
+
+
+@pytest.mark.parametrize('case', sorted(AFF_CASES))
+def test_afferent_coupling_monitors(case):
+    """AfferentCoupling / AfferentCouplingTemporalAverage (monitors.py:394-433; node_coupling of step + 1,
+    simulator.py:314-320,358-361) against reference runs: one, two and the SigmoidalJansenRit single
+    coupling row."""
+    fx = G.load('afferent_40')
+    model, cf, cp, dt, n_steps, mons = AFF_CASES[case]
+    out, _ = O.simulate(model, {}, fx['weights'], fx['tract_lengths'], float(fx['speed']), dt, cf, cp,
+                        'HeunDeterministic', n_steps, mons(), fx[case + '_buffer0'], fx[case + '_state0'], 0)
+    for k, (t, y) in enumerate(out):
+        ref = fx['%s_m%d' % (case, k)]
+        assert y.shape == ref.shape, (case, k)
+        np.testing.assert_allclose(t, fx['%s_m%d_t' % (case, k)], rtol=0, atol=1e-12)
+        err = np.abs(y - ref).max() / np.abs(ref).max()
+        assert err < 1e-9, (case, k, err)

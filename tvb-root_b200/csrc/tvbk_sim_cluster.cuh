@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const t
     if (upd) {
         node.init(L, Ip, r0 + tid, n, s0);
         if (Ip->row_ptr[r0 + tid + 1] - Ip->row_ptr[r0 + tid] > 32 * MAXE) atomicOr(status, TVBK_STATUS_DEGREE);
+        if (Ip->aff != nullptr) atomicOr(status, TVBK_STATUS_UNSUPPORTED);
     }
     float* __restrict__ raw = Ip->ring;
     // gather ring: the raw ring, or for SigmoidalJansenRit the pre-applied sigmoid values, recomputed from

@@ -262,8 +262,10 @@ struct RegRow<M, CF, 0> {
 };
 
 // Per-region state and update: scheme step with noise, ring write and the
-// monitors (shared by both kernel variants).
-template <class M, int SCHEME>
+// monitors (shared by all kernel variants).  EXT = false builds it without
+// the region stimulus and the AfferentCoupling monitor, for launches that
+// use neither (their terms and registers are then absent, not zero).
+template <class M, int SCHEME, bool EXT = true>
 struct Node {
     static constexpr int NSV = M::NSV, NCV = M::NCV, NP = M::NP, NINT = M::NINT;
     static constexpr bool STOCH = SchemeTraits<SCHEME>::stoch;
@@ -277,6 +279,9 @@ struct Node {
     float stim_w;         // this region's spatial weight
     uint32_t stim_vars;
     float* tavg_p;
+    float* aff_p;         // AfferentCoupling output row of the next sample (NULL: monitor off)
+    float aacc[NCV];      // its running sum
+    int cd_a, a_istep;    // steps to its next sample, its period
     double* bold_p;
     float* sub_p;
     int ph_t, ph_b, ph_i, ph_s, q_prev;
@@ -326,11 +331,48 @@ struct Node {
         sub_p = Ip->sub ? Ip->sub + (size_t)(s0 / Ip->sub_istep - Ip->sub_base) * nvoi * n + i : nullptr;
         raw_p = Ip->raw ? Ip->raw + (size_t)(s0 - Ip->raw_base) * nvoi * n + i : nullptr;
         fed_p = Ip->noise_fed ? Ip->noise_fed + (size_t)(s0 - Ip->fed_base) * NINT * n + i : nullptr;
-        stim_p = Ip->stim ? Ip->stim + (s0 - Ip->stim_base) : nullptr;
-        stim_w = Ip->stim ? Ip->stim_weight[i] : 0.0f;
-        stim_vars = Ip->stim ? Ip->stim_vars : 0u;
         tavg_p = do_tavg ? Ip->tavg + (size_t)(s0 / Ip->tavg_istep - Ip->tavg_base) * nvoi * n + i : nullptr;
+        if constexpr (EXT) {
+            stim_p = Ip->stim ? Ip->stim + (s0 - Ip->stim_base) : nullptr;
+            stim_w = Ip->stim ? Ip->stim_weight[i] : 0.0f;
+            stim_vars = Ip->stim ? Ip->stim_vars : 0u;
+            a_istep = Ip->aff ? Ip->aff_istep : 1;
+            aff_p = Ip->aff ? Ip->aff + (size_t)(s0 / a_istep - Ip->aff_base) * NCV * n + i : nullptr;
+            cd_a = a_istep - (int)(s0 % a_istep);
+#pragma unroll
+            for (int k = 0; k < NCV; ++k) aacc[k] = Ip->aff ? Ip->aff_acc[k * n + i] : 0.0f;
+        } else {
+            stim_p = nullptr;
+            stim_w = 0.0f;
+            stim_vars = 0u;
+            aff_p = nullptr;
+            a_istep = cd_a = 1;
+#pragma unroll
+            for (int k = 0; k < NCV; ++k) aacc[k] = 0.0f;
+        }
         bold_p = do_bold ? Ip->bold + (size_t)(s0 / Ip->bold_istep - Ip->bold_base) * nvoi * n + i : nullptr;
+    }
+
+    // AfferentCoupling after a step: cn is the coupling the next step receives
+    // (simulator.py:358-361 samples node_coupling of step + 1); the mean over
+    // the period is written when the step is a multiple of a_istep (the
+    // TemporalAverage rule, monitors.py:380-391; a_istep = 1 for Raw).
+    __device__ __forceinline__ void afferent(const float* cn, int n) {
+        // __fadd_rn: the coupling value is rounded before it is summed (no
+        // contraction with the coupling's post into an FMA), so an average
+        // taken here equals one taken on the host from the every-step stream
+#pragma unroll
+        for (int k = 0; k < NCV; ++k) aacc[k] = __fadd_rn(aacc[k], cn[k]);
+        if (--cd_a == 0) {
+            cd_a = a_istep;
+            const float inv_n = (float)a_istep;
+#pragma unroll
+            for (int k = 0; k < NCV; ++k) {
+                aff_p[k * n] = aacc[k] / inv_n;
+                aacc[k] = 0.0f;
+            }
+            aff_p += (size_t)NCV * n;
+        }
     }
 
     // Philox normals of the 4-step block of step s (steps 4q .. 4q+3, q = s >> 2).
@@ -346,6 +388,7 @@ struct Node {
 
     // Stimulus of step s0 + 1 + ks: spatial weight x temporal pattern (patterns.py:116-134).
     __device__ __forceinline__ float stim_at(int ks) const {
+        if constexpr (!EXT) return 0.0f;
         return stim_p != nullptr ? stim_w * __ldg(stim_p + ks) : 0.0f;
     }
 
@@ -358,28 +401,37 @@ struct Node {
         M::dfun(x, c, p, m0);
 #pragma unroll
         for (int k = 0; k < NSV; ++k) sv[k] = ((stim_vars >> k) & 1u) ? st : 0.0f;
+        // a + stimulus, a + dt * stimulus (the identity without EXT)
+        auto with_st = [&](float a, int k) -> float {
+            if constexpr (EXT) return a + sv[k];
+            return a;
+        };
+        auto add_dt_st = [&](float a, int k) -> float {
+            if constexpr (EXT) return a + dt * sv[k];
+            return a;
+        };
         if constexpr (SCHEME == TVBK_SCHEME_EULER_DET) {
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * (m0[k] + sv[k]);
+            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * with_st(m0[k], k);
         } else if constexpr (SCHEME == TVBK_SCHEME_EULER_STOCH) {
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + dt * m0[k] + sig[k] * z[k] + dt * sv[k];
+            for (int k = 0; k < NSV; ++k) x[k] = add_dt_st(x[k] + dt * m0[k] + sig[k] * z[k], k);
         } else if constexpr (SCHEME == TVBK_SCHEME_HEUN_DET || SCHEME == TVBK_SCHEME_HEUN_STOCH) {
             float inter[NSV], nz[NSV];
 #pragma unroll
             for (int k = 0; k < NSV; ++k) {
                 nz[k] = STOCH ? sig[k] * z[k] : 0.0f;
                 if constexpr (STOCH)
-                    inter[k] = x[k] + dt * m0[k] + nz[k] + dt * sv[k];
+                    inter[k] = add_dt_st(x[k] + dt * m0[k] + nz[k], k);
                 else
-                    inter[k] = x[k] + dt * (m0[k] + sv[k]);
+                    inter[k] = x[k] + dt * with_st(m0[k], k);
             }
             M::bound(inter);
             float m1[NSV];
             M::dfun(inter, c, p, m1);
             const float hdt = dt * 0.5f;
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = x[k] + (m0[k] + m1[k]) * hdt + nz[k] + dt * sv[k];
+            for (int k = 0; k < NSV; ++k) x[k] = add_dt_st(x[k] + (m0[k] + m1[k]) * hdt + nz[k], k);
         } else if constexpr (SCHEME == TVBK_SCHEME_RK4) {
             const float dt2 = dt * 0.5f, dt6 = dt / 6.0f;
             float st[NSV], k2[NSV], k3[NSV], k4[NSV];
@@ -397,10 +449,10 @@ struct Node {
             M::dfun(st, c, p, k4);
 #pragma unroll
             for (int k = 0; k < NSV; ++k)
-                x[k] = x[k] + dt6 * (m0[k] + 2.0f * k2[k] + 2.0f * k3[k] + k4[k]) + dt * sv[k];
+                x[k] = add_dt_st(x[k] + dt6 * (m0[k] + 2.0f * k2[k] + 2.0f * k3[k] + k4[k]), k);
         } else {  // identity
 #pragma unroll
-            for (int k = 0; k < NSV; ++k) x[k] = m0[k] + sv[k];
+            for (int k = 0; k < NSV; ++k) x[k] = with_st(m0[k], k);
         }
         M::bound(x);
     }
@@ -658,6 +710,10 @@ struct Node {
                 if (Ip->tavg != nullptr) Ip->tavg_acc[v * n + i] = tacc[v];
                 if (Ip->bold != nullptr) Ip->bold_acc[v * n + i] = bacc[v];
             }
+        if (EXT && aff_p != nullptr) {
+#pragma unroll
+            for (int k = 0; k < NCV; ++k) Ip->aff_acc[k * n + i] = aacc[k];
+        }
         if (!finite) atomicOr(status, TVBK_STATUS_NONFINITE);
     }
 };
@@ -675,7 +731,9 @@ __device__ __forceinline__ void stage_ring(float* dst, const float* src, int nfl
 // <= s - d_min only, so it does not wait for this step), which gives each
 // warp two independent instruction streams; it needs every delay >= 1, a
 // barrier interval K <= d_min, and a coupling whose pre() ignores x_i.
-template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE>
+// EXT = false: no region stimulus and no AfferentCoupling monitor (launch.extras
+// == 0); an instance that asks for either gets TVBK_STATUS_UNSUPPORTED.
+template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE, bool EXT = true>
 __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     constexpr int NCV = M::NCV;
     constexpr bool SIGMA = GatherTraits<CF, NCV>::SIGMA;
@@ -709,10 +767,11 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     }
     RegRow<M, CF, MAXD> row;
     row.deg = 0;
-    Node<M, SCHEME> node;
+    Node<M, SCHEME, EXT> node;
     if (act) {
         const int e0 = Ip->row_ptr[i], e1 = Ip->row_ptr[i + 1];
         if (MAXD > 0 && e1 - e0 > MAXD) atomicOr(L.status + blockIdx.x, TVBK_STATUS_DEGREE);
+        if (!EXT && (Ip->stim != nullptr || Ip->aff != nullptr)) atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
         row.load(Ip->edges, e0, e1);
         node.init(L, Ip, i, n, s0);
     }
@@ -744,6 +803,15 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
             if (++since_sync == K) {
                 since_sync = 0;
                 __syncthreads();
+            }
+            // AfferentCoupling: the coupling of step s + 1, gathered where the
+            // next iteration would gather it (after its barrier)
+            if (EXT && act && node.aff_p != nullptr) {
+                float cn[NCV], xi[NCV];
+#pragma unroll
+                for (int k = 0; k < NCV; ++k) xi[k] = node.x[M::cvar(k)];
+                row.couple(ring, wslot * slot_floats, ring_floats, xi, cf, cn, L.cfun);
+                node.afferent(cn, n);
             }
         }
     } else {
@@ -786,6 +854,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                         for (int k = 0; k < M::NINT; ++k) z[k] = node.zc[k][r];
                         node.integrate(c, z, L.dt, node.stim_at(ks + r));
                         node.accumulate(L, n);
+                        if (EXT && node.aff_p != nullptr) node.afferent(cnext, n);
                         write(wslot);
                     }
                     if constexpr (SchemeTraits<SCHEME>::stoch) {
@@ -815,6 +884,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                     node.fetch_z(L, n, s, z);
                     node.integrate(c, z, L.dt, node.stim_at(ks));
                     node.accumulate(L, n);
+                    if (EXT && node.aff_p != nullptr) node.afferent(cnext, n);
                     write(wslot);
                 }
                 zq = s >> 2;
@@ -909,6 +979,7 @@ __global__ void __launch_bounds__(512) sim_kernel_ep(const tvbk_launch L) {
             tl = (e1 - 1) / E;
         }
         node.init(L, Ip, t, n, s0);
+        if (Ip->aff != nullptr) atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
     }
     __syncthreads();
 
@@ -978,9 +1049,9 @@ __global__ void __launch_bounds__(512) sim_kernel_ep(const tvbk_launch L) {
 
 // ------------------------------------------------------------------ launch
 
-template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE = false>
+template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE = false, bool EXT = true>
 int launch_one(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
-    auto kern = sim_kernel<M, CF, SCHEME, SMEM, MAXT, MAXD, PIPE>;
+    auto kern = sim_kernel<M, CF, SCHEME, SMEM, MAXT, MAXD, PIPE, EXT>;
     if (smem_bytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
         if (e != cudaSuccess) return (int)e;
@@ -996,6 +1067,11 @@ int launch_deg(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes, int max
     if (max_deg <= 0) return launch_one<M, CF, SCHEME, SMEM, MAXT, 0>(L, st, smem_bytes);
     if constexpr (CF != CF_DIFFERENCE && CF != CF_GENERIC) {
         if (L.prefetch) {
+            // rings in shared memory without stimulus or AfferentCoupling: the lean build
+            if (SMEM && L.extras == 0) {
+                if (max_deg <= 32) return launch_one<M, CF, SCHEME, SMEM, MAXT, 32, true, false>(L, st, smem_bytes);
+                if (max_deg <= 64) return launch_one<M, CF, SCHEME, SMEM, MAXT, 64, true, false>(L, st, smem_bytes);
+            }
             if (max_deg <= 32) return launch_one<M, CF, SCHEME, SMEM, MAXT, 32, true>(L, st, smem_bytes);
             if (max_deg <= 64) return launch_one<M, CF, SCHEME, SMEM, MAXT, 64, true>(L, st, smem_bytes);
         }

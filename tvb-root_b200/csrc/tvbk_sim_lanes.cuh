@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel_group(const tvbk_launch L) {
         if (deg > L.max_degree) atomicOr(L.status + (size_t)blockIdx.x * G + v, TVBK_STATUS_DEGREE);
         deg = min(deg, L.max_degree);
         node.init(L, Ip, i, n, s0);
+        if (Ip->aff != nullptr) atomicOr(L.status + (size_t)blockIdx.x * G + v, TVBK_STATUS_UNSUPPORTED);
     }
     __syncthreads();
 

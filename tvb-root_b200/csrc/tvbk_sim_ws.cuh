@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(512) sim_kernel_ws(const tvbk_launch L) {
             row.load(Ip->edges, e0, e1);
         } else {
             node.init(L, Ip, i, n, s0);
+            if (Ip->aff != nullptr) atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
         }
     }
     __syncthreads();

@@ -19,6 +19,7 @@ TVBK_ERR_CUDA = -3
 TVBK_ERR_TOO_LARGE = -4
 TVBK_STATUS_NONFINITE = 1
 TVBK_STATUS_DEGREE = 2
+TVBK_STATUS_UNSUPPORTED = 4
 
 MODEL_IDS = {'Generic2dOscillator': 0, 'JansenRit': 1, 'ReducedWongWang': 2, 'Epileptor': 3, 'Sum': 4}
 CFUN_IDS = {'Linear': 0, 'Difference': 1, 'SigmoidalJansenRit': 2, 'Sigmoidal': 3, 'HyperbolicTangent': 4,
@@ -52,6 +53,8 @@ class Inst(ctypes.Structure):
         ('raw', ctypes.c_void_p),
         ('sub', ctypes.c_void_p),
         ('tavg', ctypes.c_void_p),
+        ('aff', ctypes.c_void_p),
+        ('aff_acc', ctypes.c_void_p),
         ('tavg_acc', ctypes.c_void_p),
         ('bold', ctypes.c_void_p),
         ('bold_acc', ctypes.c_void_p),
@@ -65,6 +68,7 @@ class Inst(ctypes.Structure):
         ('bold_base', ctypes.c_int64),
         ('sub_base', ctypes.c_int64),
         ('stim_base', ctypes.c_int64),
+        ('aff_base', ctypes.c_int64),
         ('n', ctypes.c_int32),
         ('nnz', ctypes.c_int32),
         ('horizon', ctypes.c_int32),
@@ -75,6 +79,7 @@ class Inst(ctypes.Structure):
         ('stock_len', ctypes.c_int32),
         ('sub_istep', ctypes.c_int32),
         ('stim_vars', ctypes.c_uint32),
+        ('aff_istep', ctypes.c_int32),
         ('cfun', ctypes.c_float * 6),
         ('seed', ctypes.c_uint32),
         ('stream', ctypes.c_uint32),
@@ -104,6 +109,7 @@ class Launch(ctypes.Structure):
         ('lanes', ctypes.c_int32),
         ('cluster', ctypes.c_int32),
         ('cluster_edges', ctypes.c_int32),
+        ('extras', ctypes.c_int32),
         ('max_steps', ctypes.c_int64),
         ('dt', ctypes.c_float),
     ]

@@ -96,7 +96,7 @@ class InstanceSpec:
     """
 
     def __init__(self, conn, ring0, state0, params, cfun, n_steps, step0=0, sigma=None, noise_fed=None,
-                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0, stim=None):
+                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0, stim=None, aff_istep=0):
         self.conn = conn
         self.ring0 = ring0
         self.state0 = state0
@@ -124,6 +124,7 @@ class InstanceSpec:
                 mask |= 1 << int(v)
             stim = dict(temporal=np.ascontiguousarray(t[:self.n_steps]), weight=np.ascontiguousarray(w), mask=mask)
         self.stim = stim
+        self.aff_istep = int(aff_istep)  # AfferentCoupling period in steps (1: every step; 0: none)
         # monitor accumulators carried over from a previous run of the same
         # simulation: dict with 'tavg_acc' (nvoi, n), 'bold_acc' (nvoi, n),
         # 'bold_stock' (stock_len, nvoi, n); None starts them at zero
@@ -152,6 +153,10 @@ class Batch:
         if self.max_n > _lib.MAX_REGIONS:
             raise ValueError('%d regions exceed this build (%d)' % (self.max_n, _lib.MAX_REGIONS))
         hmax = max(s.conn.horizon for s in self.specs)
+        # AfferentCoupling is written by the row kernel only
+        self.afferent = any(s.aff_istep for s in self.specs)
+        # launch.extras: without a stimulus or AfferentCoupling the row kernel runs its lean build
+        self.extras = (1 if any(s.stim is not None for s in self.specs) else 0) | (2 if self.afferent else 0)
         self.lanes = self._choose_lanes(lanes, gather)
         V = self.lanes
         # SigmoidalJansenRit with the row / cluster kernels gathers from a ring of pre-applied sigmoid
@@ -179,6 +184,8 @@ class Batch:
         if self.generic and (gather in ('edge', 'split') or V != 1):
             raise ValueError('Sigmoidal, HyperbolicTangent and Kuramoto run on the row gather, one instance '
                              'per CTA')
+        if self.afferent and (gather in ('edge', 'split') or V != 1):
+            raise ValueError('AfferentCoupling monitors run on the row gather, one instance per CTA')
         if gather != 'edge' and dmin >= 1 and self.cfun_id != _lib.CFUN_IDS['Difference'] \
                 and self.model_id != _lib.MODEL_IDS['Sum'] and not self.generic:
             # row kernel with the next step's gather issued ahead: barrier interval K <= d_min
@@ -231,7 +238,7 @@ class Batch:
         threads = -(-self.max_n * G // 32) * 32
         smem = -(-self.max_n * self.max_degree * 8 // 16) * 16 + 2 * self.max_degree * self.ncvar * threads * 4
         ok = (same and gather != 'edge' and self.model_id != _lib.MODEL_IDS['Sum'] and threads <= 1024
-              and self.cfun_id not in _lib.CFUN_GENERIC
+              and self.cfun_id not in _lib.CFUN_GENERIC and not self.afferent
               and smem <= 227 * 1024 and len(specs) % G == 0)
         if ok:
             return G
@@ -252,7 +259,7 @@ class Batch:
         if cluster in (None, 0, 1, '0', '1'):
             return 0, 0
         able = (self.lanes == 1 and not self.ring_in_smem and not self.edges_per_thread
-                and self.model_id != _lib.MODEL_IDS['Sum'] and not self.generic)
+                and self.model_id != _lib.MODEL_IDS['Sum'] and not self.generic and not self.afferent)
         if cluster == 'auto':
             if not able or self.max_n < 64:
                 return 0, 0
@@ -357,6 +364,8 @@ class Batch:
                 acc_arena.add(('bold_stock', k), len(h) * nvoi * n * 8)
             if s.tavg_istep:
                 acc_arena.add(('tavg_acc', k), nvoi * n * 4)
+            if s.aff_istep:
+                acc_arena.add(('aff_acc', k), self.ncvar * n * 4)
             # outputs
             s1 = s.step0 + s.n_steps
             if s.raw:
@@ -372,6 +381,9 @@ class Batch:
             if s.sub_istep:
                 m['sub_rows'] = s1 // s.sub_istep - s.step0 // s.sub_istep
                 outa.add(('sub', k), max(m['sub_rows'], 1) * nvoi * n * 4)
+            if s.aff_istep:
+                m['aff_rows'] = s1 // s.aff_istep - s.step0 // s.aff_istep
+                outa.add(('aff', k), max(m['aff_rows'], 1) * self.ncvar * n * 4)
             self.meta.append(m)
         init.add(('insts',), len(specs) * _lib.INST_DTYPE.itemsize)
         zero.add(('status',), len(specs) * 4)
@@ -448,11 +460,17 @@ class Batch:
                 d['stim_vars'] = s.stim['mask']
                 d['stim_base'] = s.step0
             if s.acc0 is not None:
-                for key, dtype in (('tavg_acc', np.float32), ('bold_acc', np.float64), ('bold_stock', np.float64)):
+                for key, dtype in (('tavg_acc', np.float32), ('bold_acc', np.float64), ('bold_stock', np.float64),
+                                   ('aff_acc', np.float32)):
                     if (key, k) in init.regions and s.acc0.get(key) is not None:
                         put((key, k), np.asarray(s.acc0[key], dtype=dtype))
             d['raw'] = zaddr(('raw', k))
             d['sub'] = zaddr(('sub', k))
+            if s.aff_istep:
+                d['aff'] = zaddr(('aff', k))
+                d['aff_acc'] = zaddr(('aff_acc', k))
+                d['aff_istep'] = s.aff_istep
+                d['aff_base'] = s.step0 // s.aff_istep
             if s.sub_istep:
                 d['sub_istep'] = s.sub_istep
                 d['sub_base'] = s.step0 // s.sub_istep
@@ -528,6 +546,7 @@ class Batch:
         L.lanes = self.lanes
         L.cluster = self.cluster
         L.cluster_edges = self.cluster_edges
+        L.extras = self.extras
         L.prefetch = self.prefetch
         L.max_steps = int(max_steps)
         L.dt = self.dt
@@ -608,6 +627,8 @@ class Batch:
             out['bold'] = self._oview(('bold', k), torch.float64, (m['bold_rows'], nvoi, m['n']))
         if 'sub_rows' in m:
             out['sub'] = self._oview(('sub', k), torch.float32, (m['sub_rows'], nvoi, m['n']))
+        if 'aff_rows' in m:
+            out['aff'] = self._oview(('aff', k), torch.float32, (m['aff_rows'], self.ncvar, m['n']))
         return out
 
     def outputs_host(self):
@@ -621,11 +642,13 @@ class Batch:
             o = {}
             nvoi, n = self.nvoi, m['n']
             for key, dt, rows in (('raw', np.float32, 'raw_rows'), ('tavg', np.float32, 'tavg_rows'),
-                                  ('bold', np.float64, 'bold_rows'), ('sub', np.float32, 'sub_rows')):
+                                  ('bold', np.float64, 'bold_rows'), ('sub', np.float32, 'sub_rows'),
+                                  ('aff', np.float32, 'aff_rows')):
                 if rows in m:
                     off, nb = self.out.regions[(key, k)]
-                    cnt = m[rows] * nvoi * n
-                    o[key] = host[off:off + nb].view(dt)[:cnt].reshape(m[rows], nvoi, n)
+                    nv = self.ncvar if key == 'aff' else nvoi
+                    cnt = m[rows] * nv * n
+                    o[key] = host[off:off + nb].view(dt)[:cnt].reshape(m[rows], nv, n)
             res.append(o)
         return res
 
@@ -640,6 +663,8 @@ class Batch:
         acc = {}
         if ('tavg_acc', k) in self.zero.regions or ('tavg_acc', k) in self.init.regions:
             acc['tavg_acc'] = self._region_view(('tavg_acc', k), torch.float32, (nvoi, m['n'])).cpu().numpy()
+        if s.aff_istep:
+            acc['aff_acc'] = self._region_view(('aff_acc', k), torch.float32, (self.ncvar, m['n'])).cpu().numpy()
         if s.bold is not None:
             acc['bold_acc'] = self._region_view(('bold_acc', k), torch.float64, (nvoi, m['n'])).cpu().numpy()
             acc['bold_stock'] = self._region_view(('bold_stock', k), torch.float64,

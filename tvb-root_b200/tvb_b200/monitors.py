@@ -1,4 +1,5 @@
-"""Raw, TemporalAverage and Bold monitors (tvb/simulator/monitors.py).
+"""Raw, TemporalAverage, Bold, SubSample, GlobalAverage, SpatialAverage and
+AfferentCoupling monitors (tvb/simulator/monitors.py).
 
 Sampling runs inside the simulation kernel; these classes resolve the step
 constants exactly as the reference does and shape the outputs.
@@ -154,4 +155,72 @@ class SpatialAverage(SubSample):
         return np.einsum('gn,tvn->tvg', self.spatial_mean, y.astype(np.float64))
 
 
-MONITORS = {cls.__name__: cls for cls in (Raw, TemporalAverage, Bold, SubSample, GlobalAverage, SpatialAverage)}
+class AfferentCoupling(Monitor):
+    """The coupling input of the model, node_coupling, recorded after every
+    step: at step s the coupling that step s + 1 receives (simulator.py:
+    314-320, 358-361; monitors.py:394-412).  variables_of_interest indexes
+    the coupling variables (default: all of the model's cvar).  Data
+    (T, nvoi, n), stamped step * dt."""
+    default_period = 0.0
+
+    def _config_vois(self, sim):
+        vois = self.variables_of_interest
+        self.voi = vois if vois is not None and vois.size else np.arange(len(sim.model.cvar))
+
+    def _config_time(self, sim):
+        self.dt = sim.integrator.dt
+        self.period = sim.integrator.dt
+        self.istep = 1
+
+    def times(self, steps):
+        return steps * self.dt
+
+
+class AfferentCouplingTemporalAverage(AfferentCoupling):
+    """AfferentCoupling averaged over each period and stamped at its middle, the
+    TemporalAverage rule (monitors.py:415-433, 363-391)."""
+
+    def _config_time(self, sim):
+        Monitor._config_time(self, sim)
+        if self.istep < 1:
+            raise ValueError('AfferentCouplingTemporalAverage needs a period of at least one step (got %g)'
+                             % self.period)
+
+    def times(self, steps):
+        return (steps - self.istep / 2.0) * self.dt
+
+    def average(self, raw, s0, carry):
+        """This monitor's samples from the every-step AfferentCoupling stream of
+        steps s0 + 1 .. s0 + T, raw (T, ncvar, n) float32, when another
+        AfferentCoupling monitor with a different period shares the run.
+        carry is the float32 sum of the current period so far.  The sums run
+        in step order in float32 and are divided by istep, the arithmetic the
+        device does for a single period.  Returns (samples (S, ncvar, n),
+        new carry)."""
+        istep, T = self.istep, raw.shape[0]
+        inv = np.float32(istep)
+        acc = np.array(carry, dtype=np.float32, copy=True)
+        out = []
+        first = (s0 // istep + 1) * istep - s0       # steps up to and including the first sample step
+        h = min(T, first)
+        for k in range(h):
+            acc = acc + raw[k]
+        if first <= T:
+            out.append(acc / inv)
+            acc = np.zeros_like(acc)
+        rest = raw[h:]
+        W = rest.shape[0] // istep
+        if W:
+            R = rest[:W * istep].reshape((W, istep) + raw.shape[1:])
+            w = np.zeros((W,) + raw.shape[1:], dtype=np.float32)
+            for j in range(istep):
+                w = w + R[:, j]
+            out.extend(w / inv)
+        for k in range(W * istep, rest.shape[0]):
+            acc = acc + rest[k]
+        samples = np.stack(out) if out else np.zeros((0,) + raw.shape[1:], dtype=np.float32)
+        return samples, acc
+
+
+MONITORS = {c.__name__: c for c in (Raw, TemporalAverage, Bold, SubSample, GlobalAverage, SpatialAverage,
+                                    AfferentCoupling, AfferentCouplingTemporalAverage)}

@@ -212,6 +212,9 @@ class SimulationServer:
         L.lanes = 1
         L.cluster = p0.cluster
         L.cluster_edges = max(p.cluster_edges for p in plans)
+        L.extras = 0
+        for p in plans:
+            L.extras |= p.extras
         L.max_steps = self.chunk_steps
         L.dt = p0.dt
         st = g.stream

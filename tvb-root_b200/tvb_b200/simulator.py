@@ -88,8 +88,10 @@ def adopt_monitor(mon):
         return monitors_mod.Raw()
     if name == 'TemporalAverage':
         return monitors_mod.TemporalAverage(period=mon.period, variables_of_interest=voi)
-    if name in ('SubSample', 'GlobalAverage'):
+    if name in ('SubSample', 'GlobalAverage', 'AfferentCouplingTemporalAverage'):
         return monitors_mod.MONITORS[name](period=mon.period, variables_of_interest=voi)
+    if name == 'AfferentCoupling':
+        return monitors_mod.AfferentCoupling(variables_of_interest=voi)
     if name == 'SpatialAverage':
         return monitors_mod.SpatialAverage(period=mon.period, variables_of_interest=voi,
                                            spatial_mask=getattr(mon, 'spatial_mask', None))
@@ -189,6 +191,11 @@ class Simulator:
         self._configure_history()
         for m in self.monitors:
             m.config_for_sim(self)
+            # node_coupling has one row per coupling variable, one for SigmoidalJansenRit (coupling.py:370-373)
+            ncrows = 1 if self._cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
+            if isinstance(m, monitors_mod.AfferentCoupling) and np.asarray(m.voi).max() >= ncrows:
+                raise IndexError('AfferentCoupling variables_of_interest %s: node_coupling has %d rows'
+                                 % (np.asarray(m.voi).tolist(), ncrows))
         self._voi_codes = self.model.voi_codes()
         if len(self._voi_codes) > _lib.MAX_VOI:
             raise NotImplementedError('more than %d variables of interest' % _lib.MAX_VOI)
@@ -198,6 +205,11 @@ class Simulator:
         if self.integrator.stochastic:
             self._sigma = noise_sigma(self.integrator.noise.nsig, self.nint, self.number_of_nodes, dt)
         self._acc = None
+        # AfferentCoupling monitors: the device averages over their period when they share one; with several
+        # periods it writes every step and the averaging monitors reduce that stream on the host
+        aff_periods = sorted({m.istep for m in self.monitors if isinstance(m, monitors_mod.AfferentCoupling)})
+        self._aff_istep = aff_periods[0] if len(aff_periods) == 1 else (1 if aff_periods else 0)
+        self._aff_carry = {}
         self._stim = None
         if self.stimulus is not None:
             if type(self.stimulus).__name__ != 'StimuliRegion':
@@ -300,7 +312,8 @@ class Simulator:
                             self.coupling.kernel_params(), n_steps, step0=self.current_step, sigma=self._sigma,
                             noise_fed=fed, seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                             stream=self.stream_id if stream is None else stream, raw=raw, tavg_istep=tavg_istep,
-                            bold=bspec, sub_istep=self._sub_istep, stim=self.stimulus_spec(n_steps))
+                            bold=bspec, sub_istep=self._sub_istep, stim=self.stimulus_spec(n_steps),
+                            aff_istep=self._aff_istep)
         if self._acc is not None:
             spec.acc0 = self._acc
         return spec, noise_kind
@@ -313,6 +326,8 @@ class Simulator:
         st = batch.status()
         if st[0] & _lib.TVBK_STATUS_NONFINITE:
             self.log_nonfinite = True
+        if st[0] & _lib.TVBK_STATUS_UNSUPPORTED:
+            raise RuntimeError('the kernel variant chosen for this simulation does not write all its monitors')
         out = batch.outputs_host()[0]
         s0 = self.current_step
         self.current_step = s0 + n_steps
@@ -326,7 +341,7 @@ class Simulator:
         """Per-monitor (times, data) in the reference's format."""
         res = []
         steps = np.arange(s0 + 1, s0 + n_steps + 1)
-        for m in self.monitors:
+        for k, m in enumerate(self.monitors):
             if isinstance(m, monitors_mod.Raw):
                 t, y = m.times(steps.astype(np.float64)), out['raw'][:, m.voi]
             elif isinstance(m, monitors_mod.TemporalAverage):
@@ -335,6 +350,17 @@ class Simulator:
             elif isinstance(m, monitors_mod.SubSample):
                 st = steps[steps % m.istep == 0]
                 t, y = m.times(st.astype(np.float64)), m.reduce(out['sub'][:, m.voi])
+            elif isinstance(m, monitors_mod.AfferentCoupling):
+                st = steps[steps % m.istep == 0]
+                if m.istep == self._aff_istep:
+                    y = out['aff'][:, m.voi]
+                else:
+                    carry = self._aff_carry.get(k)
+                    if carry is None:
+                        carry = np.zeros(out['aff'].shape[1:], dtype=np.float32)
+                    y, self._aff_carry[k] = m.average(out['aff'], s0, carry)
+                    y = y[:, m.voi]
+                t = m.times(st.astype(np.float64))
             else:
                 st = steps[steps % m.istep == 0]
                 t, y = m.times(st.astype(np.float64)), out['bold'][:, m.voi]
@@ -389,7 +415,8 @@ class Simulator:
         history (H, ncvar, n, 1) float32 and current_state (nsv, n, 1) as the
         reference's history.buffer and current_state; current_step;
         monitor_stock_<k> for the k-th monitor (1-based): Raw an empty array,
-        TemporalAverage (istep, nvoi_k, n, 1) holding the current period's sum
+        TemporalAverage and AfferentCouplingTemporalAverage (istep, nvoi_k, n, 1)
+        holding the current period's sum
         in row 0 (the reference's stock rows are only ever read as their mean
         at the next sample, which this reproduces), Bold the 4 ms stock
         (stock_len, nvoi_k, n, 1) float64; monitor_names; for stochastic
@@ -411,6 +438,13 @@ class Simulator:
                 stock = np.zeros((m.istep, voi.size, n, 1))
                 if 'tavg_acc' in acc:
                     stock[0, :, :, 0] = acc['tavg_acc'][voi]
+                st[name] = stock
+            elif isinstance(m, monitors_mod.AfferentCouplingTemporalAverage):
+                stock = np.zeros((m.istep, voi.size, n, 1))
+                if k in self._aff_carry:
+                    stock[0, :, :, 0] = self._aff_carry[k][voi]
+                elif 'aff_acc' in acc and m.istep == self._aff_istep:
+                    stock[0, :, :, 0] = acc['aff_acc'][voi]
                 st[name] = stock
             elif isinstance(m, monitors_mod.Bold):
                 SL = m.hemodynamic_response_function.shape[1]
@@ -458,6 +492,14 @@ class Simulator:
                 ph = self.current_step % m.istep
                 t[voi] = np.asarray(stock)[:ph, :, :, 0].sum(axis=0)
                 acc['tavg_acc'] = t
+            elif isinstance(m, monitors_mod.AfferentCouplingTemporalAverage) and stock is not None:
+                t = np.zeros((self.ncvar, n), dtype=np.float32)
+                ph = self.current_step % m.istep
+                t[voi] = np.asarray(stock)[:ph, :, :, 0].sum(axis=0)
+                if m.istep == self._aff_istep:
+                    acc['aff_acc'] = t
+                else:
+                    self._aff_carry[k] = t
             elif isinstance(m, monitors_mod.Bold) and stock is not None:
                 stock = np.asarray(stock)
                 b = np.zeros((stock.shape[0], nvoi, n))

@@ -123,7 +123,7 @@ class ParameterSweep:
                                 int(self.n_steps_each[i]), step0=sim.current_step, sigma=sigma, noise_fed=None,
                                 seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                                 stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep,
-                                stim=stim_i)
+                                stim=stim_i, aff_istep=sim._aff_istep)
             specs.append(spec)
         self._specs = specs
         noise_kind = _lib.NOISE_NONE
@@ -182,8 +182,9 @@ class ParameterSweep:
 
     def run(self, fc=True):
         """Build, run and return host results: dict with per-monitor arrays
-        (I, T, nvoi, n) under 'raw' / 'tavg' / 'bold' (lists of (T_i, nvoi, n)
-        arrays for uneven lengths) and 'fc' (I, n, n)."""
+        (I, T, nvoi, n) under 'raw' / 'tavg' / 'bold' / 'sub' (lists of
+        (T_i, nvoi, n) arrays for uneven lengths), 'aff' (I, T, ncvar, n) for
+        the AfferentCoupling monitors and 'fc' (I, n, n)."""
         if self.batch is None:
             self.build()
         self.run_device()
@@ -191,7 +192,7 @@ class ParameterSweep:
         if fc and any(isinstance(m, monitors_mod.Bold) for m in self.monitors):
             res['fc'] = self.fc_device().cpu().numpy()
         outs = self.batch.outputs_host()
-        for key in ('raw', 'tavg', 'bold', 'sub'):
+        for key in ('raw', 'tavg', 'bold', 'sub', 'aff'):
             if key in outs[0]:
                 arrs = [o[key] for o in outs]
                 # instances of uneven lengths give a list of (T_i, nvoi, n) arrays
