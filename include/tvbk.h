@@ -51,8 +51,9 @@ extern "C" {
 /* per-instance status bits written by the simulation kernel */
 #define TVBK_STATUS_NONFINITE 1   /* a state variable became NaN or Inf */
 #define TVBK_STATUS_DEGREE 2      /* a row had more edges than launch.max_degree (coupling incomplete) */
-#define TVBK_STATUS_UNSUPPORTED 4 /* the instance asks for an output this kernel variant does not write
-                                   * (AfferentCoupling on a variant other than the row kernel) */
+#define TVBK_STATUS_UNSUPPORTED 4 /* the instance asks for something this kernel variant does not do
+                                   * (AfferentCoupling on a variant other than the row kernel; a stimulus,
+                                   * AfferentCoupling or projection stream with launch.extras = 0) */
 
 /* components */
 enum {
@@ -136,6 +137,10 @@ typedef struct tvbk_inst {
                                   * s + 1 receives, taken after step s and averaged over aff_istep steps (1: every
                                   * step); sample s / aff_istep - aff_base - 1.  Row kernel only */
     float* aff_acc;              /* [ncvar][n] running sum of the current aff_istep period */
+    float* proj;                 /* [*][nvoi][n] projection monitors (EEG / MEG / iEEG, monitors.py:436-831): the
+                                  * mean of the observed variables over each proj_istep steps, sample
+                                  * s / proj_istep - proj_base - 1; the host applies the sensor gain (a GEMM) */
+    float* proj_acc;             /* [nvoi][n] running sum of the current proj_istep period */
     float* tavg_acc;             /* [nvoi][n] running sum of the current period */
     double* bold;                /* [*][nvoi][n]; sample s / bold_istep - bold_base - 1 */
     double* bold_acc;            /* [nvoi][n] running sum of the current 4 ms window */
@@ -143,11 +148,11 @@ typedef struct tvbk_inst {
     const double* hrf;           /* [stock_len] reversed haemodynamic kernel */
     int64_t step;                /* last completed step (the reference's current_step) */
     int64_t step_end;            /* run until step == step_end */
-    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base, stim_base, aff_base;
+    int64_t raw_base, fed_base, tavg_base, bold_base, sub_base, stim_base, aff_base, proj_base;
     int32_t n, nnz, horizon, ring_len;
     int32_t tavg_istep, bold_istep, bold_ii, stock_len, sub_istep;
     uint32_t stim_vars;          /* bit k: state variable k receives the stimulus (the model's stvar) */
-    int32_t aff_istep;
+    int32_t aff_istep, proj_istep;
     float cfun[6];               /* coupling parameters, see tvbk_sim_run */
     uint32_t seed, stream;       /* Philox key */
     double bold_k1v0;            /* k_1 * V_0 of the FirstOrderVolterra kernel */
@@ -190,9 +195,9 @@ typedef struct tvbk_launch {
     int32_t cluster_edges;       /* cluster kernel: edges of one CTA's rows that it stages in shared memory; a CTA
                                   * with more edges reads them from global memory (0: always global) */
     int32_t extras;              /* bit 0: some instance has a region stimulus; bit 1: some instance has an
-                                  * AfferentCoupling monitor.  0 lets the row kernel with rings in shared memory
-                                  * use a build without either (an instance that has one then gets
-                                  * TVBK_STATUS_UNSUPPORTED) */
+                                  * AfferentCoupling monitor; bit 2: some instance has a projection stream.  0
+                                  * lets the row kernel with rings in shared memory use a build without any of
+                                  * them (an instance that has one then gets TVBK_STATUS_UNSUPPORTED) */
     int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */
     float dt;
 } tvbk_launch;

@@ -333,8 +333,13 @@ def iround(x):
 
 
 class Monitor:
-    def __init__(self, kind, period=None, voi=None, spatial_mask=None):
+    """kind, period, voi; SpatialAverage: spatial_mask; Projection (EEG / MEG /
+    iEEG): gain (sensors, n), obs_z (one (sensors, nvoi) standard-normal draw
+    per sample, or None) and ref_vec (sensors,) for the EEG reference."""
+
+    def __init__(self, kind, period=None, voi=None, spatial_mask=None, gain=None, obs_z=None, ref_vec=None):
         self.kind, self.period, self.voi, self.spatial_mask = kind, period, voi, spatial_mask
+        self.gain, self.obs_z, self.ref_vec = gain, obs_z, ref_vec
 
 
 def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, coupling_params,
@@ -432,6 +437,10 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
                 total[np.arange(nn), m.spatial_mask] = 1
                 total = total.T
                 st['mean'] = total / np.sum(total, axis=1)[:, np.newaxis]
+        elif m.kind == 'Projection':                     # monitors.py:596-600
+            st['istep'] = int(m.period / dt)
+            st['state'] = np.zeros((m.gain.shape[0], len(mv)))
+            st['k'] = 0
         elif m.kind == 'Bold':
             st['istep'] = iround(m.period / dt)
             st['ii'] = int(round((1.0 / 2.0 ** -2) / dt))
@@ -512,6 +521,19 @@ def simulate(model, model_params, weights, tract_lengths, speed, dt, coupling, c
                         st['y'].append(np.mean(o, axis=1)[:, np.newaxis])
                     else:                                  # monitors.py:321-325 (o is (nvoi, n): no modes axis)
                         st['y'].append(np.dot(st['mean'], o.T).T)
+            elif m.kind == 'Projection':                 # monitors.py:602-614, EEG 718-723
+                st['state'] += m.gain.dot(o.T)
+                if step % st['istep'] == 0:
+                    sample = st['state'].copy() / st['istep']
+                    if m.obs_z is not None:
+                        sample += np.sqrt(dt) * m.obs_z[st['k']]
+                    st['k'] += 1
+                    st['state'][:] = 0.0
+                    sample = sample.T
+                    if m.ref_vec is not None:
+                        sample = sample - m.ref_vec.dot(sample.T)[:, np.newaxis]
+                    st['t'].append((step - st['istep'] / 2.0) * dt)
+                    st['y'].append(sample)
             elif m.kind == 'Bold':                       # monitors.py:942-962
                 ii = st['ii']
                 st['interim'][(step % ii) - 1] = o

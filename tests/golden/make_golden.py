@@ -63,12 +63,13 @@ def import_reference(ref):
     import tvb.simulator.noise as noise
     import tvb.simulator.history as history
     from tvb.datatypes.connectivity import Connectivity
-    from tvb.datatypes import equations, patterns
+    from tvb.datatypes import equations, patterns, sensors, projections, region_mapping
     from tvb.basic.neotraits.api import List
     return dict(simulator=simulator, models=models, coupling=coupling,
                 integrators=integrators, monitors=monitors, noise=noise,
                 history=history, Connectivity=Connectivity, List=List,
-                equations=equations, patterns=patterns)
+                equations=equations, patterns=patterns, sensors=sensors, projections=projections,
+                region_mapping=region_mapping)
 
 
 FP64_FIELDS = {
@@ -655,6 +656,82 @@ def case_afferent(R):
     save('afferent_40', **out)
 
 
+def case_projection(R):
+    """EEG / MEG / iEEG monitors on Generic2dOscillator (the 40-region
+    connectome of case_couplings, Linear a=0.0152, HeunDeterministic dt 0.1,
+    40 ms) with seeded synthetic sensors, region centres / orientations and
+    lead fields over a 200-vertex source space: EEG (16 sensors, average
+    reference, default observation noise) and MEG (12 sensors, no
+    observation noise) at period 1000/1024 ms (9 steps); iEEG (10 sensors,
+    observation noise, 4 non-cortical regions with the analytic lead field)
+    alone at period 2 ms."""
+    w, L = synthetic_connectome(40, 0.40, 10.0, 120.0, seed=21)
+    speed = 3.0
+    n, V = 40, 200
+    rng = np.random.default_rng(41)
+    centres = rng.normal(size=(n, 3)) * 30.0
+    ori = rng.normal(size=(n, 3))
+    ori /= np.sqrt((ori ** 2).sum(axis=1))[:, None]
+    rmap = np.concatenate([np.arange(n), rng.integers(0, n, V - n)])
+    cortical = np.ones(n, dtype=bool)
+    cortical[[3, 11, 27, 38]] = False
+    sens = {k: rng.normal(size=(S, 3)) * 90.0 for k, S in (('eeg', 16), ('meg', 12), ('ieeg', 10))}
+    lead = {'eeg': rng.normal(size=(16, V)), 'meg': rng.normal(size=(12, V)) * 1e-3,
+            'ieeg': rng.normal(size=(10, int((~np.isin(rmap, np.flatnonzero(~cortical))).sum())))}
+    out = dict(weights=w, tract_lengths=L, speed=speed, centres=centres, orientations=ori, rmap=rmap,
+               cortical=cortical, **{'sensors_' + k: v for k, v in sens.items()},
+               **{'lead_' + k: v for k, v in lead.items()})
+    S_, P_, RM, Mo = R['sensors'], R['projections'], R['region_mapping'], R['monitors']
+
+    def conn(with_cortical):
+        c = make_conn(R, w, L, speed)
+        c.centres = centres
+        c.orientations = ori
+        c.cortical = cortical if with_cortical else np.ones(n, dtype=bool)
+        return c
+
+    def labels(k, S):
+        return np.array(['%s%d' % (k, i) for i in range(S)])
+
+    cases = {
+        'em': (False, lambda c: [
+            Mo.EEG(period=1e3 / 1024.0, sensors=S_.SensorsEEG(labels=labels('e', 16), locations=sens['eeg']),
+                   projection=P_.ProjectionSurfaceEEG(projection_data=lead['eeg']),
+                   region_mapping=RM.RegionMapping(array_data=rmap, connectivity=c), reference='average'),
+            Mo.MEG(period=1e3 / 1024.0, sensors=S_.SensorsMEG(labels=labels('m', 12), locations=sens['meg'],
+                                                               orientations=np.tile([0.0, 0.0, 1.0], (12, 1))),
+                   projection=P_.ProjectionSurfaceMEG(projection_data=lead['meg']),
+                   region_mapping=RM.RegionMapping(array_data=rmap, connectivity=c), obsnoise=None)], 501),
+        'ieeg': (True, lambda c: [
+            Mo.iEEG(period=2.0, sensors=S_.SensorsInternal(labels=labels('i', 10), locations=sens['ieeg']),
+                    projection=P_.ProjectionSurfaceSEEG(projection_data=lead['ieeg']),
+                    region_mapping=RM.RegionMapping(array_data=rmap, connectivity=c))], 502),
+    }
+    for name, (with_cortical, mons, seed) in cases.items():
+        def build(with_cortical=with_cortical, mons=mons):
+            c = conn(with_cortical)
+            return R['simulator'].Simulator(
+                model=R['models'].Generic2dOscillator(), connectivity=c,
+                coupling=R['coupling'].Linear(a=np.array([0.0152])),
+                integrator=R['integrators'].HeunDeterministic(dt=0.1), monitors=mons(c), simulation_length=40.0)
+        sim, cfg, res, _, _ = run_sim(R, build, 40.0, False, ic_seed=seed)
+        out[name + '_buffer0'] = cfg['buffer0']
+        out[name + '_state0'] = cfg['state0']
+        for k, (t, y) in enumerate(res):
+            out['%s_m%d' % (name, k)] = y[..., 0]
+            out['%s_m%d_t' % (name, k)] = t
+            out['%s_m%d_gain' % (name, k)] = np.array(sim.monitors[k].gain)
+    # the analytic lead fields (Sarvas 1987) on their own, for 8 sources
+    src, so = centres[:8], ori[:8]
+    out['eeg_analytic'] = Mo.EEG(sensors=S_.SensorsEEG(labels=labels('e', 16), locations=sens['eeg']),
+                                 sigma=0.7).analytic(src, so)
+    out['meg_analytic'] = Mo.MEG(sensors=S_.SensorsMEG(labels=labels('m', 12), locations=sens['meg'],
+                                                       orientations=np.tile([0.0, 0.0, 1.0], (12, 1)))).analytic(src, so)
+    out['ieeg_analytic'] = Mo.iEEG(sensors=S_.SensorsInternal(labels=labels('i', 10), locations=sens['ieeg']),
+                                   sigma=0.7).analytic(src, so)
+    save('projection_40', **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference/tvb_library')
@@ -686,6 +763,7 @@ def main():
         'balloon': lambda: case_balloon(R),
         'stimulus': lambda: case_stimulus(R),
         'afferent': lambda: case_afferent(R),
+        'projection': lambda: case_projection(R),
     }
     for name, fn in cases.items():
         if args.only and name not in args.only:

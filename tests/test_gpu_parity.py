@@ -660,3 +660,73 @@ def test_afferent_coupling_stays_on_the_row_kernel():
     res = ParameterSweep(**kw, lanes='auto', cluster='auto').configure().run(fc=False)
     assert (res['status'] == 0).all()
     assert res['aff'].shape == (4, 20, 1, 68)
+
+
+def _projection_monitors(fx):
+    from tvb_b200 import monitors, sensors
+    from tvb_b200.sensors import ProjectionSurfaceEEG, ProjectionSurfaceMEG, ProjectionSurfaceSEEG, RegionMapping
+
+    def labels(k, S):
+        return ['%s%d' % (k, i) for i in range(S)]
+    em = [monitors.EEG(period=1e3 / 1024.0, sensors=sensors.SensorsEEG(labels('e', 16), fx['sensors_eeg']),
+                       projection=ProjectionSurfaceEEG(fx['lead_eeg']), region_mapping=RegionMapping(fx['rmap']),
+                       reference='average'),
+          monitors.MEG(period=1e3 / 1024.0, sensors=sensors.SensorsMEG(labels('m', 12), fx['sensors_meg']),
+                       projection=ProjectionSurfaceMEG(fx['lead_meg']), region_mapping=RegionMapping(fx['rmap']),
+                       obsnoise=None)]
+    ieeg = [monitors.iEEG(period=2.0, sensors=sensors.SensorsInternal(labels('i', 10), fx['sensors_ieeg']),
+                          projection=ProjectionSurfaceSEEG(fx['lead_ieeg']), region_mapping=RegionMapping(fx['rmap']))]
+    return em, ieeg
+
+
+@pytest.mark.parametrize('case', ['em', 'ieeg'])
+def test_projection_monitors_vs_reference(case):
+    """EEG (average reference, observation noise), MEG and iEEG (analytic lead field of non-cortical regions) on
+    the device -- period means of the observed variables in the kernel, the lead field applied as a float64 GEMM
+    on the device -- against the reference's runs; 137-step chunks give the same samples."""
+    from tvb_b200 import coupling, integrators, models
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.simulator import Simulator
+    fx = G.load('projection_40')
+
+    def make(chunk):
+        em, ieeg = _projection_monitors(fx)
+        conn = Connectivity(fx['weights'], fx['tract_lengths'], speed=float(fx['speed']), centres=fx['centres'],
+                            orientations=fx['orientations'], cortical=fx['cortical'] if case == 'ieeg' else None)
+        np.random.seed(501 if case == 'em' else 502)
+        return Simulator(model=models.Generic2dOscillator(), connectivity=conn, coupling=coupling.Linear(a=0.0152),
+                         integrator=integrators.HeunDeterministic(dt=0.1), monitors=em if case == 'em' else ieeg,
+                         simulation_length=40.0, chunk_steps=chunk).configure()
+    sim = make(200000)
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx[case + '_buffer0'])
+    res = sim.run()
+    for k, (t, y) in enumerate(res):
+        np.testing.assert_allclose(t, fx['%s_m%d_t' % (case, k)], rtol=0, atol=1e-12)
+        report('projection %s m%d vs reference' % (case, k), y[..., 0], fx['%s_m%d' % (case, k)], 1e-4)
+    for (t, y), (t2, y2) in zip(res, make(137).run()):
+        np.testing.assert_array_equal(t, t2)
+        np.testing.assert_allclose(y, y2, rtol=1e-12, atol=1e-12)
+
+
+def test_projection_sweep_matches_simulator():
+    """ParameterSweep's EEG signals (one GEMM over all instances) equal each instance's own Simulator run."""
+    from tvb_b200 import coupling, integrators, models
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.simulator import Simulator
+    from tvb_b200.sweep import ParameterSweep
+    fx = G.load('projection_40')
+    conn = Connectivity(fx['weights'], fx['tract_lengths'], speed=float(fx['speed']))
+    a = np.array([0.005, 0.0152, 0.03])
+    np.random.seed(501)
+    sw = ParameterSweep(model=models.Generic2dOscillator(), connectivity=conn, coupling=coupling.Linear(),
+                        integrator=integrators.HeunDeterministic(dt=0.1), monitors=_projection_monitors(fx)[0][:1],
+                        simulation_length=40.0, sweep={'coupling.a': a}).configure()
+    res = sw.run(fc=False)
+    assert (res['status'] == 0).all()
+    for i in (0, 2):
+        np.random.seed(501)
+        sim = Simulator(model=models.Generic2dOscillator(), connectivity=conn, coupling=coupling.Linear(a=a[i]),
+                        integrator=integrators.HeunDeterministic(dt=0.1), monitors=_projection_monitors(fx)[0][:1],
+                        simulation_length=40.0).configure()
+        (t, y), = sim.run()
+        report('projection sweep instance %d vs Simulator' % i, res['projection'][0][i], y[..., 0], 1e-5)

@@ -334,3 +334,31 @@ def test_afferent_coupling_monitors(case):
         np.testing.assert_allclose(t, fx['%s_m%d_t' % (case, k)], rtol=0, atol=1e-12)
         err = np.abs(y - ref).max() / np.abs(ref).max()
         assert err < 1e-9, (case, k, err)
+
+
+def test_projection_monitors():
+    """EEG (average reference, observation noise), MEG and iEEG (analytic lead field for non-cortical regions)
+    sampled every int(period / dt) steps (monitors.py:436-831) against reference runs, with the reference's
+    configured gains and its observation-noise stream (RandomState(42), one (sensors, nvoi) draw per sample)."""
+    fx = G.load('projection_40')
+    w, L = fx['weights'], fx['tract_lengths']
+
+    def obs(S, T):
+        rs = np.random.RandomState(42)
+        return [rs.normal(size=(S, 1)) for _ in range(T)]
+    mons = [O.Monitor('Projection', 1e3 / 1024.0, gain=fx['em_m0_gain'], obs_z=obs(16, 44), ref_vec=np.full(16, 1 / 16)),
+            O.Monitor('Projection', 1e3 / 1024.0, gain=fx['em_m1_gain'])]
+    out, _ = O.simulate('Generic2dOscillator', {}, w, L, float(fx['speed']), 0.1, 'Linear', {'a': 0.0152},
+                        'HeunDeterministic', 400, mons, fx['em_buffer0'], fx['em_state0'], 0)
+    for k, (t, y) in enumerate(out):
+        ref = fx['em_m%d' % k]
+        assert y.shape == ref.shape
+        np.testing.assert_allclose(t, fx['em_m%d_t' % k], rtol=0, atol=1e-12)
+        assert np.abs(y - ref).max() / np.abs(ref).max() < 1e-9, k
+    out, _ = O.simulate('Generic2dOscillator', {}, w, L, float(fx['speed']), 0.1, 'Linear', {'a': 0.0152},
+                        'HeunDeterministic', 400,
+                        [O.Monitor('Projection', 2.0, gain=fx['ieeg_m0_gain'], obs_z=obs(10, 20))],
+                        fx['ieeg_buffer0'], fx['ieeg_state0'], 0)
+    (t, y), = out
+    np.testing.assert_allclose(t, fx['ieeg_m0_t'], rtol=0, atol=1e-12)
+    assert np.abs(y - fx['ieeg_m0']).max() / np.abs(fx['ieeg_m0']).max() < 1e-9

@@ -282,6 +282,9 @@ struct Node {
     float* aff_p;         // AfferentCoupling output row of the next sample (NULL: monitor off)
     float aacc[NCV];      // its running sum
     int cd_a, a_istep;    // steps to its next sample, its period
+    float* proj_p;        // projection stream row of the next sample (NULL: off)
+    float pacc[MV];       // its running sums
+    int cd_p, p_istep;
     double* bold_p;
     float* sub_p;
     int ph_t, ph_b, ph_i, ph_s, q_prev;
@@ -341,6 +344,11 @@ struct Node {
             cd_a = a_istep - (int)(s0 % a_istep);
 #pragma unroll
             for (int k = 0; k < NCV; ++k) aacc[k] = Ip->aff ? Ip->aff_acc[k * n + i] : 0.0f;
+            p_istep = Ip->proj ? Ip->proj_istep : 1;
+            proj_p = Ip->proj ? Ip->proj + (size_t)(s0 / p_istep - Ip->proj_base) * nvoi * n + i : nullptr;
+            cd_p = p_istep - (int)(s0 % p_istep);
+#pragma unroll
+            for (int v = 0; v < MV; ++v) pacc[v] = (Ip->proj && v < nvoi) ? Ip->proj_acc[v * n + i] : 0.0f;
         } else {
             stim_p = nullptr;
             stim_w = 0.0f;
@@ -349,6 +357,10 @@ struct Node {
             a_istep = cd_a = 1;
 #pragma unroll
             for (int k = 0; k < NCV; ++k) aacc[k] = 0.0f;
+            proj_p = nullptr;
+            p_istep = cd_p = 1;
+#pragma unroll
+            for (int v = 0; v < MV; ++v) pacc[v] = 0.0f;
         }
         bold_p = do_bold ? Ip->bold + (size_t)(s0 / Ip->bold_istep - Ip->bold_base) * nvoi * n + i : nullptr;
     }
@@ -372,6 +384,32 @@ struct Node {
                 aacc[k] = 0.0f;
             }
             aff_p += (size_t)NCV * n;
+        }
+    }
+
+    // Projection stream after a step: the mean of the observed variables over
+    // p_istep steps, written when the step is a multiple of p_istep.  The
+    // sensor gain is linear, so gain . mean equals the reference's per-step
+    // gain products summed over the period and divided by it
+    // (monitors.py:602-614); the host applies it.
+    __device__ __forceinline__ void project(const tvbk_launch& L, int n) {
+        if constexpr (EXT) {
+            if (proj_p == nullptr) return;
+            const int nvoi = L.nvoi;
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) pacc[v] += M::observe(L.voi[v], x);
+            if (--cd_p == 0) {
+                cd_p = p_istep;
+                const float inv_n = (float)p_istep;
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) {
+                        proj_p[v * n] = pacc[v] / inv_n;
+                        pacc[v] = 0.0f;
+                    }
+                proj_p += (size_t)nvoi * n;
+            }
         }
     }
 
@@ -544,6 +582,7 @@ struct Node {
                 if (v < nvoi) sub_p[v * n] = M::observe(L.voi[v], x);
             sub_p += (size_t)nvoi * n;
         }
+        project(L, n);
     }
 
     // ---- pieces of a step for the row kernel's blocked loop ----------------
@@ -589,6 +628,7 @@ struct Node {
             for (int v = 0; v < MV; ++v)
                 if (v < nvoi) bacc[v] += (double)M::observe(L.voi[v], x);
         }
+        project(L, n);
     }
 
     // Advance the clock by m steps, the last of which is step s, and take the
@@ -714,6 +754,11 @@ struct Node {
 #pragma unroll
             for (int k = 0; k < NCV; ++k) Ip->aff_acc[k * n + i] = aacc[k];
         }
+        if (EXT && proj_p != nullptr) {
+#pragma unroll
+            for (int v = 0; v < MV; ++v)
+                if (v < nvoi) Ip->proj_acc[v * n + i] = pacc[v];
+        }
         if (!finite) atomicOr(status, TVBK_STATUS_NONFINITE);
     }
 };
@@ -771,7 +816,8 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     if (act) {
         const int e0 = Ip->row_ptr[i], e1 = Ip->row_ptr[i + 1];
         if (MAXD > 0 && e1 - e0 > MAXD) atomicOr(L.status + blockIdx.x, TVBK_STATUS_DEGREE);
-        if (!EXT && (Ip->stim != nullptr || Ip->aff != nullptr)) atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
+        if (!EXT && (Ip->stim != nullptr || Ip->aff != nullptr || Ip->proj != nullptr))
+            atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
         row.load(Ip->edges, e0, e1);
         node.init(L, Ip, i, n, s0);
     }

@@ -55,6 +55,8 @@ class Inst(ctypes.Structure):
         ('tavg', ctypes.c_void_p),
         ('aff', ctypes.c_void_p),
         ('aff_acc', ctypes.c_void_p),
+        ('proj', ctypes.c_void_p),
+        ('proj_acc', ctypes.c_void_p),
         ('tavg_acc', ctypes.c_void_p),
         ('bold', ctypes.c_void_p),
         ('bold_acc', ctypes.c_void_p),
@@ -69,6 +71,7 @@ class Inst(ctypes.Structure):
         ('sub_base', ctypes.c_int64),
         ('stim_base', ctypes.c_int64),
         ('aff_base', ctypes.c_int64),
+        ('proj_base', ctypes.c_int64),
         ('n', ctypes.c_int32),
         ('nnz', ctypes.c_int32),
         ('horizon', ctypes.c_int32),
@@ -80,6 +83,7 @@ class Inst(ctypes.Structure):
         ('sub_istep', ctypes.c_int32),
         ('stim_vars', ctypes.c_uint32),
         ('aff_istep', ctypes.c_int32),
+        ('proj_istep', ctypes.c_int32),
         ('cfun', ctypes.c_float * 6),
         ('seed', ctypes.c_uint32),
         ('stream', ctypes.c_uint32),

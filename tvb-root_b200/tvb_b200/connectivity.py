@@ -6,7 +6,8 @@ from . import _lib
 
 
 class Connectivity:
-    def __init__(self, weights, tract_lengths, speed=None, region_labels=None, centres=None):
+    def __init__(self, weights, tract_lengths, speed=None, region_labels=None, centres=None, orientations=None,
+                 cortical=None):
         self.weights = np.asarray(weights, dtype=np.float64)
         self.tract_lengths = np.asarray(tract_lengths, dtype=np.float64)
         if self.weights.ndim != 2 or self.weights.shape[0] != self.weights.shape[1]:
@@ -15,7 +16,10 @@ class Connectivity:
             raise ValueError('tract_lengths must have the shape of weights')
         self.speed = None if speed is None else np.atleast_1d(np.asarray(speed, dtype=np.float64))
         self.region_labels = region_labels
-        self.centres = centres
+        self.centres = None if centres is None else np.asarray(centres, dtype=np.float64)
+        # source positions and unit orientations, and the cortical mask, used by the projection monitors
+        self.orientations = None if orientations is None else np.asarray(orientations, dtype=np.float64)
+        self.cortical = np.zeros(0, dtype=bool) if cortical is None else np.asarray(cortical, dtype=bool)
         self.delays = None
         self.idelays = None
         self._horizon = None

@@ -96,7 +96,8 @@ class InstanceSpec:
     """
 
     def __init__(self, conn, ring0, state0, params, cfun, n_steps, step0=0, sigma=None, noise_fed=None,
-                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0, stim=None, aff_istep=0):
+                 seed=42, stream=0, raw=False, tavg_istep=0, bold=None, sub_istep=0, stim=None, aff_istep=0,
+                 proj_istep=0):
         self.conn = conn
         self.ring0 = ring0
         self.state0 = state0
@@ -125,6 +126,7 @@ class InstanceSpec:
             stim = dict(temporal=np.ascontiguousarray(t[:self.n_steps]), weight=np.ascontiguousarray(w), mask=mask)
         self.stim = stim
         self.aff_istep = int(aff_istep)  # AfferentCoupling period in steps (1: every step; 0: none)
+        self.proj_istep = int(proj_istep)  # projection-monitor period in steps (0: none)
         # monitor accumulators carried over from a previous run of the same
         # simulation: dict with 'tavg_acc' (nvoi, n), 'bold_acc' (nvoi, n),
         # 'bold_stock' (stock_len, nvoi, n); None starts them at zero
@@ -156,7 +158,8 @@ class Batch:
         # AfferentCoupling is written by the row kernel only
         self.afferent = any(s.aff_istep for s in self.specs)
         # launch.extras: without a stimulus or AfferentCoupling the row kernel runs its lean build
-        self.extras = (1 if any(s.stim is not None for s in self.specs) else 0) | (2 if self.afferent else 0)
+        self.extras = ((1 if any(s.stim is not None for s in self.specs) else 0) | (2 if self.afferent else 0)
+                       | (4 if any(s.proj_istep for s in self.specs) else 0))
         self.lanes = self._choose_lanes(lanes, gather)
         V = self.lanes
         # SigmoidalJansenRit with the row / cluster kernels gathers from a ring of pre-applied sigmoid
@@ -366,6 +369,8 @@ class Batch:
                 acc_arena.add(('tavg_acc', k), nvoi * n * 4)
             if s.aff_istep:
                 acc_arena.add(('aff_acc', k), self.ncvar * n * 4)
+            if s.proj_istep:
+                acc_arena.add(('proj_acc', k), nvoi * n * 4)
             # outputs
             s1 = s.step0 + s.n_steps
             if s.raw:
@@ -384,6 +389,9 @@ class Batch:
             if s.aff_istep:
                 m['aff_rows'] = s1 // s.aff_istep - s.step0 // s.aff_istep
                 outa.add(('aff', k), max(m['aff_rows'], 1) * self.ncvar * n * 4)
+            if s.proj_istep:
+                m['proj_rows'] = s1 // s.proj_istep - s.step0 // s.proj_istep
+                outa.add(('proj', k), max(m['proj_rows'], 1) * nvoi * n * 4)
             self.meta.append(m)
         init.add(('insts',), len(specs) * _lib.INST_DTYPE.itemsize)
         zero.add(('status',), len(specs) * 4)
@@ -461,7 +469,7 @@ class Batch:
                 d['stim_base'] = s.step0
             if s.acc0 is not None:
                 for key, dtype in (('tavg_acc', np.float32), ('bold_acc', np.float64), ('bold_stock', np.float64),
-                                   ('aff_acc', np.float32)):
+                                   ('aff_acc', np.float32), ('proj_acc', np.float32)):
                     if (key, k) in init.regions and s.acc0.get(key) is not None:
                         put((key, k), np.asarray(s.acc0[key], dtype=dtype))
             d['raw'] = zaddr(('raw', k))
@@ -471,6 +479,11 @@ class Batch:
                 d['aff_acc'] = zaddr(('aff_acc', k))
                 d['aff_istep'] = s.aff_istep
                 d['aff_base'] = s.step0 // s.aff_istep
+            if s.proj_istep:
+                d['proj'] = zaddr(('proj', k))
+                d['proj_acc'] = zaddr(('proj_acc', k))
+                d['proj_istep'] = s.proj_istep
+                d['proj_base'] = s.step0 // s.proj_istep
             if s.sub_istep:
                 d['sub_istep'] = s.sub_istep
                 d['sub_base'] = s.step0 // s.sub_istep
@@ -629,6 +642,8 @@ class Batch:
             out['sub'] = self._oview(('sub', k), torch.float32, (m['sub_rows'], nvoi, m['n']))
         if 'aff_rows' in m:
             out['aff'] = self._oview(('aff', k), torch.float32, (m['aff_rows'], self.ncvar, m['n']))
+        if 'proj_rows' in m:
+            out['proj'] = self._oview(('proj', k), torch.float32, (m['proj_rows'], nvoi, m['n']))
         return out
 
     def outputs_host(self):
@@ -643,7 +658,7 @@ class Batch:
             nvoi, n = self.nvoi, m['n']
             for key, dt, rows in (('raw', np.float32, 'raw_rows'), ('tavg', np.float32, 'tavg_rows'),
                                   ('bold', np.float64, 'bold_rows'), ('sub', np.float32, 'sub_rows'),
-                                  ('aff', np.float32, 'aff_rows')):
+                                  ('aff', np.float32, 'aff_rows'), ('proj', np.float32, 'proj_rows')):
                 if rows in m:
                     off, nb = self.out.regions[(key, k)]
                     nv = self.ncvar if key == 'aff' else nvoi
@@ -665,6 +680,8 @@ class Batch:
             acc['tavg_acc'] = self._region_view(('tavg_acc', k), torch.float32, (nvoi, m['n'])).cpu().numpy()
         if s.aff_istep:
             acc['aff_acc'] = self._region_view(('aff_acc', k), torch.float32, (self.ncvar, m['n'])).cpu().numpy()
+        if s.proj_istep:
+            acc['proj_acc'] = self._region_view(('proj_acc', k), torch.float32, (nvoi, m['n'])).cpu().numpy()
         if s.bold is not None:
             acc['bold_acc'] = self._region_view(('bold_acc', k), torch.float64, (nvoi, m['n'])).cpu().numpy()
             acc['bold_stock'] = self._region_view(('bold_stock', k), torch.float64,

@@ -224,3 +224,217 @@ class AfferentCouplingTemporalAverage(AfferentCoupling):
 
 MONITORS = {c.__name__: c for c in (Raw, TemporalAverage, Bold, SubSample, GlobalAverage, SpatialAverage,
                                     AfferentCoupling, AfferentCouplingTemporalAverage)}
+
+
+def _array(obj, attr):
+    """obj.<attr> for the reference's datatypes (and this package's), or obj itself for a plain array."""
+    return np.asarray(getattr(obj, attr, obj))
+
+
+class Projection(Monitor):
+    """Lead-field monitors (monitors.py:436-643) for region simulations.
+
+    The reference adds gain . observed state at every step and samples the
+    sum over int(period / dt) steps divided by that count.  The gain is
+    linear, so the device keeps the mean of the observed variables over each
+    period (one float32 stream for all projection monitors of a run) and the
+    sensor projection is a float64 GEMM on the device over all samples.
+    Observation noise (sqrt(dt) times a normal draw of the monitor's own
+    RandomState per sample, (sensors, nvoi) in order) is added on the host in
+    sample order, so it is the reference's stream.
+
+    sensors: object with labels / locations / usable (or the reference's
+    Sensors); projection: object with projection_data (sensors, vertices) or
+    an array; region_mapping: object with array_data (vertices,) or an array;
+    obsnoise: 'default' (white, RandomState(42)), None, or an object with
+    random_stream and ntau == 0.
+    """
+    default_period = 1e3 / 1024.0
+
+    def __init__(self, period=None, variables_of_interest=None, sensors=None, projection=None, region_mapping=None,
+                 obsnoise='default'):
+        super().__init__(period, variables_of_interest)
+        self.sensors = sensors
+        self.projection = projection
+        self.region_mapping = region_mapping
+        if obsnoise == 'default':
+            from .noise import Additive
+            obsnoise = Additive()
+        if obsnoise is not None and float(getattr(obsnoise, 'ntau', 0.0)) > 0.0:
+            raise NotImplementedError('coloured observation noise is not supported')
+        self.obsnoise = obsnoise
+        self.gain = None
+
+    def analytic(self, loc, ori):
+        raise NotImplementedError('no general analytic lead field; give a projection matrix')
+
+    def _config_time(self, sim):
+        # the reference samples every int(period / dt) steps (monitors.py:600), not iround(period / dt)
+        self.dt = sim.integrator.dt
+        self.istep = int(self.period / self.dt)
+        if self.istep < 1:
+            raise ValueError('%s period %g is shorter than dt' % (type(self).__name__, self.period))
+
+    def config_for_sim(self, sim):
+        """The region lead field (monitors.py:492-600): vertex gains summed per
+        region through the region mapping (cortical regions), the analytic
+        lead field for non-cortical regions, unusable sensors and non-finite
+        entries zeroed."""
+        super().config_for_sim(sim)
+        if self.sensors is None:
+            raise ValueError('%s needs sensors' % type(self).__name__)
+        if hasattr(self.sensors, 'configure'):
+            self.sensors.configure()
+        if self.obsnoise is not None and hasattr(self.obsnoise, 'configure_white'):
+            self.obsnoise.configure_white(dt=self.dt)
+        conn = sim.connectivity
+        n = conn.number_of_regions
+        cortical = np.asarray(getattr(conn, 'cortical', np.zeros(0)), dtype=bool)
+        if cortical.size == 0:
+            cortical = np.ones(n, dtype=bool)
+        non_cortical, = np.where(~cortical)
+        cortical_idx, = np.where(cortical)
+        if self.region_mapping is None:
+            raise ValueError('Please specify a region mapping on the EEG/MEG/iEEG monitor when performing a '
+                             'region simulation.')
+        if self.projection is None:
+            raise ValueError('%s needs a projection matrix' % type(self).__name__)
+        rmap = _array(self.region_mapping, 'array_data').astype(np.int64)
+        gain = np.array(_array(self.projection, 'projection_data'), dtype=np.float64)
+        cortical_rmap = rmap.copy()
+        if rmap.max() + 1 != cortical.sum():
+            drop = np.hstack([np.argwhere(rmap == i)[:, 0] for i in non_cortical])
+            cortical_rmap = np.delete(cortical_rmap, drop)
+        if gain.shape[1] == cortical_rmap.size:
+            g = np.zeros((gain.shape[0], n))
+            np.add.at(g.T, cortical_rmap, gain.T)
+            gain = g
+        if non_cortical.size:
+            src = (np.asarray(conn.centres)[non_cortical], np.asarray(conn.orientations)[non_cortical])
+            sub_gain = self.analytic(*src)
+            if gain.shape[1] == cortical_idx.size + non_cortical.size:
+                gain[:, non_cortical] = sub_gain
+            else:
+                full = np.zeros((gain.shape[0], gain.shape[1] + sub_gain.shape[1]))
+                full[:, cortical_idx] = gain
+                full[:, non_cortical] = sub_gain
+                gain = full
+        if gain.shape[1] != n:
+            raise ValueError('lead field has %d sources for %d regions' % (gain.shape[1], n))
+        usable = getattr(self.sensors, 'usable', None)
+        if usable is not None and not np.asarray(usable).all():
+            gain[~np.asarray(usable, dtype=bool)] = 0.0
+        gain[~np.isfinite(gain)] = 0.0
+        self.gain = gain
+        return self
+
+    def times(self, steps):
+        return (steps - self.istep / 2.0) * self.dt
+
+    def finish(self, y):
+        """(T, nvoi, S) noise-free projections -> this monitor's samples: the
+        observation noise of each sample in order, then post()."""
+        y = np.array(y, dtype=np.float64)
+        if self.obsnoise is not None:
+            rs = self.obsnoise.random_stream
+            for t in range(y.shape[0]):
+                y[t] += (np.sqrt(self.dt) * rs.normal(size=(y.shape[2], y.shape[1]))).T
+        return self.post(y)
+
+    def post(self, y):
+        return y
+
+
+class EEG(Projection):
+    """EEG (monitors.py:646-729): reference = None (reference-free), a sensor
+    label, or 'average'.  The analytic lead field of non-cortical regions is
+    the single-sphere formula of Sarvas (1987), Eq. 12."""
+
+    def __init__(self, period=None, variables_of_interest=None, sensors=None, projection=None, region_mapping=None,
+                 obsnoise='default', reference=None, sigma=1.0):
+        super().__init__(period, variables_of_interest, sensors, projection, region_mapping, obsnoise)
+        self.reference = reference
+        self.sigma = float(sigma)
+
+    def config_for_sim(self, sim):
+        super().config_for_sim(sim)
+        S = self.gain.shape[0]
+        ref = np.zeros(S)
+        if self.reference:
+            if self.reference.lower() != 'average':
+                ref[list(np.asarray(self.sensors.labels).tolist()).index(self.reference)] = 1.0
+            else:
+                ref[:] = 1.0 / S
+        self._ref_mask = np.isfinite(self.gain).all(axis=1)
+        self._ref_vec = ref[self._ref_mask]
+        return self
+
+    def analytic(self, loc, ori):
+        """Potential of unit dipoles at loc with orientation ori on sensors
+        projected to a sphere 1.05125 times the sources' radius around their
+        centre: Q . a / |a|^3 / (4 pi sigma)."""
+        centre = np.mean(loc, axis=0)[None]
+        radius = 1.05125 * max(np.sqrt(np.sum((loc - centre) ** 2, axis=1)))
+        sen = np.array(self.sensors.locations, dtype=np.float64)
+        sen = sen / np.sqrt(np.sum(sen ** 2, axis=1))[:, None] * radius + centre
+        out = np.zeros((sen.shape[0], loc.shape[0]))
+        for k in range(sen.shape[0]):
+            a = sen[k] - loc
+            na = np.sqrt(np.sum(a ** 2, axis=1))[:, None]
+            out[k] = np.sum(ori * (a / na ** 3), axis=1) / (4.0 * np.pi * self.sigma)
+        return out
+
+    def post(self, y):
+        r = np.tensordot(y[:, :, self._ref_mask], self._ref_vec, axes=([2], [0]))   # (T, nvoi)
+        return y - r[:, :, None]
+
+
+class MEG(Projection):
+    """MEG (monitors.py:732-790); non-cortical regions use the single-sphere
+    magnetic lead field of Sarvas (1987), Eq. 25."""
+
+    def analytic(self, loc, ori):
+        """|B| of unit dipoles (loc, ori) at sensors projected to a sphere 1.01
+        times the sources' radius around their centre, with
+        B = mu0 / (4 pi F^2) (F Q x r0 - (Q x r0 . r) grad F)."""
+        mu_0 = 1.25663706e-6
+        r0, Q = loc, ori
+        centre = np.mean(r0, axis=0)[None, :]
+        radius = 1.01 * max(np.sqrt(np.sum((r0 - centre) ** 2, axis=1)))
+        sen = np.array(self.sensors.locations, dtype=np.float64)
+        sen = sen / np.sqrt(np.sum(sen ** 2, axis=1))[:, None] * radius + centre
+        B = np.zeros((sen.shape[0], r0.shape[0], 3))
+        for k in range(sen.shape[0]):
+            r = sen[k][None, :]
+            a = r - r0
+            na = np.sqrt(np.sum(a ** 2, axis=1))[:, None]
+            nr = np.sqrt(np.sum(r ** 2, axis=1))[:, None]
+            F = a * (nr * a + nr ** 2 - np.sum(r0 * r, axis=1)[:, None])
+            adotr = np.sum((a / na) * r, axis=1)[:, None]
+            gradF = (na ** 2 / nr + adotr + 2.0 * na + 2.0 * nr) * r - (a + 2.0 * nr + adotr * r0)
+            B[k] = (mu_0 / (4.0 * np.pi * F ** 2)) * (np.cross(F * Q, r0)
+                                                       - np.sum(np.cross(Q, r0) * (r * gradF), axis=1)[:, None])
+        return np.sqrt(np.sum(B ** 2, axis=2))
+
+
+class iEEG(Projection):
+    """Intracranial EEG (monitors.py:793-831); non-cortical regions use the
+    point dipole in a homogeneous medium at the sensors' own positions,
+    Q . a / |a|^3 / (4 pi sigma)."""
+
+    def __init__(self, period=None, variables_of_interest=None, sensors=None, projection=None, region_mapping=None,
+                 obsnoise='default', sigma=1.0):
+        super().__init__(period, variables_of_interest, sensors, projection, region_mapping, obsnoise)
+        self.sigma = float(sigma)
+
+    def analytic(self, loc, ori):
+        sen = np.array(self.sensors.locations, dtype=np.float64)
+        out = np.zeros((sen.shape[0], loc.shape[0]))
+        for k in range(sen.shape[0]):
+            a = sen[k] - loc
+            na = np.sqrt(np.sum(a ** 2, axis=1))[:, None]
+            out[k] = np.sum(ori * (a / na ** 3), axis=1) / (4.0 * np.pi * self.sigma)
+        return out
+
+
+MONITORS.update({c.__name__: c for c in (EEG, MEG, iEEG)})

@@ -92,6 +92,14 @@ def adopt_monitor(mon):
         return monitors_mod.MONITORS[name](period=mon.period, variables_of_interest=voi)
     if name == 'AfferentCoupling':
         return monitors_mod.AfferentCoupling(variables_of_interest=voi)
+    if name in ('EEG', 'MEG', 'iEEG'):
+        kw = dict(period=mon.period, variables_of_interest=voi, sensors=mon.sensors, projection=mon.projection,
+                  region_mapping=mon.region_mapping, obsnoise=mon.obsnoise)
+        if name == 'EEG':
+            kw.update(reference=mon.reference, sigma=mon.sigma)
+        elif name == 'iEEG':
+            kw.update(sigma=mon.sigma)
+        return monitors_mod.MONITORS[name](**kw)
     if name == 'SpatialAverage':
         return monitors_mod.SpatialAverage(period=mon.period, variables_of_interest=voi,
                                            spatial_mask=getattr(mon, 'spatial_mask', None))
@@ -108,8 +116,21 @@ def adopt_monitor(mon):
 def adopt_connectivity(conn):
     if isinstance(conn, Connectivity):
         return conn
+    cort = getattr(conn, 'cortical', None)
     return Connectivity(weights=conn.weights, tract_lengths=conn.tract_lengths,
-                        speed=getattr(conn, 'speed', None))
+                        speed=getattr(conn, 'speed', None), centres=getattr(conn, 'centres', None),
+                        orientations=getattr(conn, 'orientations', None),
+                        cortical=None if cort is None or np.asarray(cort).size == 0 else cort)
+
+
+def project_samples(proj, m):
+    """(T, nvoi_m, S) = gain . mean for the device stream proj (T, nvoi, n)
+    float32 of window means and projection monitor m: a float64 GEMM on the
+    device over all samples at once."""
+    import torch
+    g = torch.as_tensor(m.gain, dtype=torch.float64, device=proj.device)          # (S, n)
+    x = proj[:, torch.as_tensor(np.asarray(m.voi), device=proj.device)].to(torch.float64)
+    return torch.matmul(x, g.T)
 
 
 def noise_sigma(nsig, nintvar, n, dt):
@@ -282,10 +303,12 @@ class Simulator:
         tavg = [m for m in self.monitors if isinstance(m, monitors_mod.TemporalAverage)]
         bold = [m for m in self.monitors if isinstance(m, monitors_mod.Bold)]
         sub = [m for m in self.monitors if isinstance(m, monitors_mod.SubSample)]
+        proj = [m for m in self.monitors if isinstance(m, monitors_mod.Projection)]
         if len(set(m.istep for m in tavg)) > 1 or len(set(m.istep for m in bold)) > 1 or \
-                len(set(m.istep for m in sub)) > 1:
+                len(set(m.istep for m in sub)) > 1 or len(set(m.istep for m in proj)) > 1:
             raise NotImplementedError('monitors of one kind must share their period')
         self._sub_istep = sub[0].istep if sub else 0
+        self._proj_istep = proj[0].istep if proj else 0
         bspec = None
         if bold:
             b = bold[0]
@@ -313,7 +336,7 @@ class Simulator:
                             noise_fed=fed, seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                             stream=self.stream_id if stream is None else stream, raw=raw, tavg_istep=tavg_istep,
                             bold=bspec, sub_istep=self._sub_istep, stim=self.stimulus_spec(n_steps),
-                            aff_istep=self._aff_istep)
+                            aff_istep=self._aff_istep, proj_istep=self._proj_istep)
         if self._acc is not None:
             spec.acc0 = self._acc
         return spec, noise_kind
@@ -329,6 +352,12 @@ class Simulator:
         if st[0] & _lib.TVBK_STATUS_UNSUPPORTED:
             raise RuntimeError('the kernel variant chosen for this simulation does not write all its monitors')
         out = batch.outputs_host()[0]
+        if self._proj_istep:
+            # the sensor projection of every sample: one float64 GEMM per monitor on the device
+            dev = batch.outputs_device(0)['proj']
+            for k, m in enumerate(self.monitors):
+                if isinstance(m, monitors_mod.Projection):
+                    out['proj_gain_%d' % k] = project_samples(dev, m).cpu().numpy()
         s0 = self.current_step
         self.current_step = s0 + n_steps
         self.current_state = batch.state(0).astype(np.float64)[..., None]
@@ -350,6 +379,9 @@ class Simulator:
             elif isinstance(m, monitors_mod.SubSample):
                 st = steps[steps % m.istep == 0]
                 t, y = m.times(st.astype(np.float64)), m.reduce(out['sub'][:, m.voi])
+            elif isinstance(m, monitors_mod.Projection):
+                st = steps[steps % m.istep == 0]
+                t, y = m.times(st.astype(np.float64)), m.finish(out['proj_gain_%d' % k])
             elif isinstance(m, monitors_mod.AfferentCoupling):
                 st = steps[steps % m.istep == 0]
                 if m.istep == self._aff_istep:
@@ -422,7 +454,10 @@ class Simulator:
         (stock_len, nvoi_k, n, 1) float64; monitor_names; for stochastic
         schemes the noise RandomState as integrator_noise_rng_state_*.  Also
         monitor_interim_<k>, Bold's running 4 ms sum (nvoi_k, n, 1), which the
-        reference does not store (it restarts that average on reload).
+        reference does not store (it restarts that average on reload).  EEG /
+        MEG / iEEG: the stock is the reference's running gain . observed sum
+        (sensors, nvoi_k) and monitor_interim_<k> the observed sum (nvoi_k, n)
+        that resuming needs; the observation-noise RandomState is not stored.
         """
         if not self._configured:
             raise RuntimeError('call configure() first')
@@ -446,6 +481,13 @@ class Simulator:
                 elif 'aff_acc' in acc and m.istep == self._aff_istep:
                     stock[0, :, :, 0] = acc['aff_acc'][voi]
                 st[name] = stock
+            elif isinstance(m, monitors_mod.Projection):
+                # the reference's running sum of gain . observed (sensors, nvoi), and the observed sum itself
+                interim = np.zeros((voi.size, n), dtype=np.float32)
+                if 'proj_acc' in acc:
+                    interim = acc['proj_acc'][voi]
+                st[name] = m.gain.dot(interim.astype(np.float64).T)
+                st['monitor_interim_%d' % (k + 1)] = interim.copy()
             elif isinstance(m, monitors_mod.Bold):
                 SL = m.hemodynamic_response_function.shape[1]
                 stock = np.zeros((SL, voi.size, n, 1))
@@ -500,6 +542,16 @@ class Simulator:
                     acc['aff_acc'] = t
                 else:
                     self._aff_carry[k] = t
+            elif isinstance(m, monitors_mod.Projection) and stock is not None:
+                interim = st.get('monitor_interim_%d' % (k + 1))
+                if interim is None:
+                    if self.current_step % m.istep and np.any(np.asarray(stock)):
+                        raise NotImplementedError('resuming %s inside a sampling period needs monitor_interim_%d'
+                                                  % (type(m).__name__, k + 1))
+                    interim = np.zeros((voi.size, n))
+                t = acc.get('proj_acc', np.zeros((nvoi, n), dtype=np.float32))
+                t[voi] = np.asarray(interim, dtype=np.float32)
+                acc['proj_acc'] = t
             elif isinstance(m, monitors_mod.Bold) and stock is not None:
                 stock = np.asarray(stock)
                 b = np.zeros((stock.shape[0], nvoi, n))

@@ -123,7 +123,7 @@ class ParameterSweep:
                                 int(self.n_steps_each[i]), step0=sim.current_step, sigma=sigma, noise_fed=None,
                                 seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
                                 stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep,
-                                stim=stim_i, aff_istep=sim._aff_istep)
+                                stim=stim_i, aff_istep=sim._aff_istep, proj_istep=sim._proj_istep)
             specs.append(spec)
         self._specs = specs
         noise_kind = _lib.NOISE_NONE
@@ -137,6 +137,26 @@ class ParameterSweep:
         return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
                      sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
                      ring_in_smem=ring_in_smem, gather=gather, lanes=lanes, cluster=cluster)
+
+    def projection(self, mons):
+        """Sensor signals of projection monitors `mons` for all instances: one
+        float64 GEMM per monitor on the device over every instance's period
+        means, then each instance's observation noise from the monitor's
+        RandomState at its current state (what separate runs would each draw)."""
+        from .simulator import project_samples
+        dev = torch.stack([self.batch.outputs_device(i)['proj'] for i in range(self.n_instances)])
+        I, T = dev.shape[:2]
+        out = []
+        for m in mons:
+            y = project_samples(dev.reshape((I * T,) + dev.shape[2:]), m).cpu().numpy().reshape(I, T, len(m.voi), -1)
+            rs = getattr(m.obsnoise, 'random_stream', None)
+            st0 = rs.get_state() if rs is not None else None
+            for i in range(I):
+                if rs is not None:
+                    rs.set_state(st0)
+                y[i] = m.finish(y[i])
+            out.append(y)
+        return out
 
     def build(self):
         """Allocate the device batch and upload inputs (one host-to-device copy).
@@ -184,7 +204,11 @@ class ParameterSweep:
         """Build, run and return host results: dict with per-monitor arrays
         (I, T, nvoi, n) under 'raw' / 'tavg' / 'bold' / 'sub' (lists of
         (T_i, nvoi, n) arrays for uneven lengths), 'aff' (I, T, ncvar, n) for
-        the AfferentCoupling monitors and 'fc' (I, n, n)."""
+        the AfferentCoupling monitors, 'proj' (I, T, nvoi, n) the period means
+        of the EEG / MEG / iEEG monitors and 'projection' (one (I, T, nvoi_m, S)
+        array per such monitor, in monitor order: the sensor signals, each
+        instance with the observation noise a separate run would draw) and
+        'fc' (I, n, n)."""
         if self.batch is None:
             self.build()
         self.run_device()
@@ -192,7 +216,10 @@ class ParameterSweep:
         if fc and any(isinstance(m, monitors_mod.Bold) for m in self.monitors):
             res['fc'] = self.fc_device().cpu().numpy()
         outs = self.batch.outputs_host()
-        for key in ('raw', 'tavg', 'bold', 'sub', 'aff'):
+        proj_mons = [m for m in self.monitors if isinstance(m, monitors_mod.Projection)]
+        if proj_mons and len({s.n_steps for s in self._specs}) == 1:
+            res['projection'] = self.projection(proj_mons)
+        for key in ('raw', 'tavg', 'bold', 'sub', 'aff', 'proj'):
             if key in outs[0]:
                 arrs = [o[key] for o in outs]
                 # instances of uneven lengths give a list of (T_i, nvoi, n) arrays
