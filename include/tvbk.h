@@ -113,6 +113,11 @@ typedef struct tvbk_inst {
     /* connectome: rows are target regions, edges in the reference's row-major non-zero order */
     const int32_t* row_ptr;      /* [n+1] */
     const tvbk_edge* edges;      /* [nnz] packed offsets and weights (tvbk_pack_edges) */
+    const tvbk_edge* slots;      /* [n][slot_width] or NULL: the row kernel's gather slots of each row -- the
+                                  * row's edges in an order where the 32 rows of a warp read distinct shared-
+                                  * memory banks in every slot (needs ring_len * n a multiple of 32), padding
+                                  * slots with weight 0; used when slot_width equals the kernel's register
+                                  * slot count, else the packed edges are read */
     /* dynamic state */
     float* ring;                 /* [ring_len][n][ncvar] */
     float* pre_ring;             /* [ring_len][n] SigmoidalJansenRit with the row or cluster kernel and rings
@@ -153,6 +158,7 @@ typedef struct tvbk_inst {
     int32_t tavg_istep, bold_istep, bold_ii, stock_len, sub_istep;
     uint32_t stim_vars;          /* bit k: state variable k receives the stimulus (the model's stvar) */
     int32_t aff_istep, proj_istep;
+    int32_t slot_width;
     float cfun[6];               /* coupling parameters, see tvbk_sim_run */
     uint32_t seed, stream;       /* Philox key */
     double bold_k1v0;            /* k_1 * V_0 of the FirstOrderVolterra kernel */

@@ -1,0 +1,58 @@
+"""Bank-conflict-free gather slots of the row kernel (CPU): every row's edges
+appear once with their offsets and weights, padding has weight 0 and reads
+at least d_min steps back, and in every slot the 32 rows of a warp read 32
+different shared-memory banks at every step and ring position."""
+import numpy as np
+import pytest
+
+
+@pytest.mark.parametrize('n,density,seed', [(68, 0.3, 3), (76, 0.4, 1), (96, 0.25, 7), (40, 0.5, 2)])
+def test_slot_table_is_a_conflict_free_permutation(n, density, seed):
+    from tvb_b200 import _lib, synthetic
+    from tvb_b200.engine import Connectome
+    w, L = synthetic.connectome(n, density, 10.0, 200.0, seed=seed)
+    idl, H = _lib.idelays(L, 5.0, 0.1)
+    c = Connectome(w, idl, 1)
+    width = 32 if np.diff(c.row_ptr).max() <= 32 else 64
+    t = c.slot_table(width)
+    assert t is not None and t.shape == (n, width, 2)
+    off = c.idelay.astype(np.int64) * n - c.col
+    wbits = c.weight.astype(np.float32).view(np.int32)
+    for r in range(n):
+        e = np.arange(c.row_ptr[r], c.row_ptr[r + 1])
+        real = t[r, :, 1] != 0
+        got = sorted(zip(t[r, real, 0].tolist(), t[r, real, 1].tolist()))
+        assert got == sorted(zip(off[e].tolist(), wbits[e].tolist()))
+        assert (t[r, ~real, 0] >= c.min_delay * n).all()
+    m = 32 // np.gcd(n, 32)
+    RL = -(-(H + 20) // m) * m
+    ring = RL * n
+    assert ring % 32 == 0
+    for base_slot in (0, 1, 17, RL - 1):
+        base = base_slot * n
+        for w0 in range(0, n, 32):
+            for k in range(width):
+                a = base - t[w0:w0 + 32, k, 0].astype(np.int64)
+                a = np.where(a < 0, a + ring, a)
+                assert ((a >= 0) & (a < ring)).all()
+                words = {}
+                for x in a.tolist():
+                    words.setdefault(x % 32, set()).add(x)
+                assert max(len(v) for v in words.values()) == 1
+
+
+def test_batch_pads_the_ring_and_keeps_two_ctas_per_sm():
+    from tvb_b200 import _lib, synthetic
+    from tvb_b200.engine import Batch, Connectome, InstanceSpec
+    n = 68
+    w, L = synthetic.connectome(n, 0.3, 10.0, 200.0, seed=3)
+    idl, H = _lib.idelays(L, 5.0, 0.1)
+    c = Connectome(w, idl, 1)
+    spec = InstanceSpec(c, np.zeros((H, 1, n), np.float32), np.zeros((1, n)), np.zeros((9, n), np.float32),
+                        [0.1, 0.0], 100, sigma=np.full((1, n), 0.01, np.float32))
+    b = Batch(_lib.MODEL_IDS['ReducedWongWang'], _lib.CFUN_IDS['Linear'], _lib.SCHEME_IDS['EulerStochastic'],
+              _lib.NOISE_PHILOX, 0.1, [0], [spec], device='cpu', allocate=False)
+    assert b.ring_in_smem and b.prefetch == 1 and b.slot_width == 32
+    RL = b.meta[0]['ring_len']
+    assert RL >= H + b.sync_every and RL * n % 32 == 0
+    assert 228 * 1024 // (RL * n * 4 + 1024) == 2

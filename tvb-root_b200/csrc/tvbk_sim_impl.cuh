@@ -169,6 +169,18 @@ struct RegRow {
         }
     }
 
+    // all MAXD slots of row r from a slot table (bank-scheduled edges and padding)
+    __device__ __forceinline__ void load_slots(const tvbk_edge* __restrict__ slots, int r, int e0, int e1) {
+        deg = e1 - e0;
+        const int2* s2 = reinterpret_cast<const int2*>(slots) + (size_t)r * MAXD;
+#pragma unroll
+        for (int k = 0; k < MAXD; ++k) {
+            const int2 ed = __ldg(s2 + k);
+            off[k] = ed.x * (int)sizeof(float);
+            w[k] = __int_as_float(ed.y);
+        }
+    }
+
     // a0 = sum over the row of w * pre (two partial sums: even / odd slots)
     template <int GCF, int NG>
     __device__ __forceinline__ void sum(const float* __restrict__ ring, int base_off, int ring_floats,
@@ -818,7 +830,14 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         if (MAXD > 0 && e1 - e0 > MAXD) atomicOr(L.status + blockIdx.x, TVBK_STATUS_DEGREE);
         if (!EXT && (Ip->stim != nullptr || Ip->aff != nullptr || Ip->proj != nullptr))
             atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
-        row.load(Ip->edges, e0, e1);
+        if constexpr (MAXD > 0) {
+            if (Ip->slots != nullptr && Ip->slot_width == MAXD)
+                row.load_slots(Ip->slots, i, e0, e1);
+            else
+                row.load(Ip->edges, e0, e1);
+        } else {
+            row.load(Ip->edges, e0, e1);
+        }
         node.init(L, Ip, i, n, s0);
     }
     const int K = L.sync_every;

@@ -42,6 +42,7 @@ class Inst(ctypes.Structure):
     _fields_ = [
         ('row_ptr', ctypes.c_void_p),
         ('edges', ctypes.c_void_p),
+        ('slots', ctypes.c_void_p),
         ('ring', ctypes.c_void_p),
         ('pre_ring', ctypes.c_void_p),
         ('state', ctypes.c_void_p),
@@ -84,6 +85,7 @@ class Inst(ctypes.Structure):
         ('stim_vars', ctypes.c_uint32),
         ('aff_istep', ctypes.c_int32),
         ('proj_istep', ctypes.c_int32),
+        ('slot_width', ctypes.c_int32),
         ('cfun', ctypes.c_float * 6),
         ('seed', ctypes.c_uint32),
         ('stream', ctypes.c_uint32),

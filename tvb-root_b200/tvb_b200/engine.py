@@ -81,6 +81,94 @@ class Connectome:
             self._packed[ncvar] = _lib.pack_edges(self.col, self.idelay, self.weight, self.n, ncvar)
         return self._packed[ncvar]
 
+    def slot_table(self, width):
+        """The row kernel's gather slots for a ring of one float per (slot,
+        region) whose length times n is a multiple of 32: (n, width, 2) int32
+        [offset, weight bits], or None when no bank-conflict-free order fits."""
+        key = ('slots', width)
+        if key not in self._packed:
+            self._packed[key] = bank_slot_table(self.row_ptr, self.col, self.idelay, self.weight, self.n, width,
+                                                self.min_delay)
+        return self._packed[key]
+
+
+def _colour_warp(lane_edges, width):
+    """Edge colouring of the bipartite multigraph lanes x banks (one edge per
+    gather edge, from its lane to its bank) with at most `width` colours: each
+    colour is a slot in which the lanes read distinct banks.  A bipartite
+    multigraph of largest degree D has a D-colouring (Koenig's edge colouring
+    theorem); it is built edge by edge, and when the free colours a (at the
+    lane) and b (at the bank) differ the a/b alternating path from the bank is
+    swapped first.  Returns {edge: colour} or None when D > width."""
+    lane_c = [dict() for _ in lane_edges]         # lane -> colour -> (bank, edge)
+    bank_c = [dict() for _ in range(32)]          # bank -> colour -> (lane, edge)
+    load = np.zeros(32, dtype=np.int64)
+    for es in lane_edges:
+        for b, _ in es:
+            load[b] += 1
+    if max(max((len(es) for es in lane_edges), default=0), int(load.max())) > width:
+        return None
+    tabs = {'lane': lane_c, 'bank': bank_c}
+    for lane, es in enumerate(lane_edges):
+        for b, e in es:
+            a = next(c for c in range(width) if c not in lane_c[lane])
+            if a in bank_c[b]:
+                c2 = next(c for c in range(width) if c not in bank_c[b])
+                path, node, side, col = [], b, 'bank', a
+                while col in tabs[side][node]:
+                    other, eid = tabs[side][node][col]
+                    path.append((side, node, other, eid, col))
+                    node, side = other, ('lane' if side == 'bank' else 'bank')
+                    col = c2 if col == a else a
+                for side, node, other, eid, col in path:
+                    oside = 'lane' if side == 'bank' else 'bank'
+                    del tabs[side][node][col]
+                    del tabs[oside][other][col]
+                for side, node, other, eid, col in path:
+                    oside = 'lane' if side == 'bank' else 'bank'
+                    nc = c2 if col == a else a
+                    tabs[side][node][nc] = (other, eid)
+                    tabs[oside][other][nc] = (node, eid)
+            lane_c[lane][a] = (b, e)
+            bank_c[b][a] = (lane, e)
+    return {e: c for lc in lane_c for c, (_, e) in lc.items()}
+
+
+def bank_slot_table(row_ptr, col, idelay, weight, n, width, dmin):
+    """Slot table for the row kernel (one float per ring entry): row r's
+    edges placed in slots 0..width-1 so that in every slot the 32 rows of a
+    warp read 32 different shared-memory banks.  The address of edge e at
+    step s is base(s) - off_e with off_e = d_e n - col_e; when the ring's
+    float count is a multiple of 32 its bank is bank(base) + (col_e - d_e n)
+    mod 32 whether or not it wraps, so a per-warp schedule holds at every
+    step.  A slot without an edge reads, with weight 0, one word of a bank no
+    edge of that slot uses (one address for all such lanes: a broadcast), at
+    least dmin steps back, where no thread of the window writes."""
+    off = idelay.astype(np.int64) * n - col.astype(np.int64)
+    bank = (-off) % 32
+    wbits = np.asarray(weight, dtype=np.float32).view(np.int32)
+    table = np.zeros((n, width, 2), dtype=np.int32)
+    for w0 in range(0, n, 32):
+        rows = range(w0, min(n, w0 + 32))
+        lane_edges = [[(int(bank[e]), e) for e in range(row_ptr[r], row_ptr[r + 1])] for r in rows]
+        colour = _colour_warp(lane_edges, width)
+        if colour is None:
+            return None
+        used = np.zeros((width, 32), dtype=bool)
+        filled = np.zeros((len(rows), width), dtype=bool)
+        for li, r in enumerate(rows):
+            for b, e in lane_edges[li]:
+                k = colour[e]
+                assert not used[k, b] and not filled[li, k]
+                used[k, b] = filled[li, k] = True
+                table[r, k] = (off[e], wbits[e])
+        for k in range(width):
+            free = int(np.flatnonzero(~used[k])[0]) if not used[k].all() else 0
+            for li, r in enumerate(rows):
+                if not filled[li, k]:
+                    table[r, k] = (dmin * n + (-free - dmin * n) % 32, 0)
+    return table
+
 
 class InstanceSpec:
     """One simulation instance.
@@ -209,6 +297,7 @@ class Batch:
             elif gather == 'edge':
                 raise ValueError('the edge-parallel gather does not apply to this batch')
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
+        self.slot_width, self._ring_len = self._choose_slots()
         self._plan()
         self.allocated = False
         if allocate:
@@ -248,6 +337,37 @@ class Batch:
         if lanes != 'auto':
             raise ValueError('these instances cannot run as groups of %d' % G)
         return 1
+
+    SM_SMEM = 228 * 1024       # shared memory of an SM
+    CTA_RESERVED = 1024        # per-CTA shared memory the hardware reserves
+
+    def _choose_slots(self):
+        """Bank-conflict-free gather slots for the row kernel with rings in
+        shared memory (one float per ring entry, 32..256 regions): the ring
+        of each instance is lengthened to the next multiple of 32 / gcd(n, 32)
+        slots (its float count then a multiple of 32), when that keeps the
+        same number of CTAs per SM.  Returns (slot width or 0, ring length of a
+        spec)."""
+        K = self.sync_every
+
+        def plain(s):
+            return s.conn.horizon + K
+        if not (self.ring_in_smem and self.lanes == 1 and not self.edges_per_thread and self.prefetch != 2
+                and self.ncvar_gather == 1 and not self.cluster and 0 < self.max_degree <= 64
+                and all(s.conn.n >= 32 for s in self.specs)):
+            return 0, plain
+        width = 32 if self.max_degree <= 32 else 64
+
+        def padded(s):
+            m = 32 // math.gcd(s.conn.n, 32)
+            return -(-(s.conn.horizon + K) // m) * m
+        old = max(plain(s) for s in self.specs) * self.max_n * 4
+        new = max(padded(s) for s in self.specs) * self.max_n * 4
+        if new > 227 * 1024 or self.SM_SMEM // (new + self.CTA_RESERVED) < self.SM_SMEM // (old + self.CTA_RESERVED):
+            return 0, plain
+        if any(s.conn.slot_table(width) is None for s in self.specs):
+            return 0, plain
+        return width, padded
 
     CLUSTER_SMEM = 227 * 1024
     CLUSTER_MAX_ROWS = 480
@@ -338,12 +458,14 @@ class Batch:
                 c = s.conn
                 conns[id(s.conn)] = c
                 init.add(('row_ptr', id(c)), c.row_ptr.nbytes)
+                if self.slot_width:
+                    init.add(('slots', id(c)), c.slot_table(self.slot_width).nbytes)
                 init.add(('edges', id(c)), max(c.edges.nbytes, 8))
         hrfs = {}
         self.meta = []
         for k, s in enumerate(specs):
             n = s.conn.n
-            RL = s.conn.horizon + self.sync_every
+            RL = self._ring_len(s)
             m = dict(n=n, ring_len=RL)
             V = self.lanes
             if k % V == 0:
@@ -430,6 +552,8 @@ class Batch:
             cptr[key] = (put(('row_ptr', key), c.row_ptr), put(('edges', key), c.packed(self.ncvar_gather))
                          if c.nnz else ib + init.regions[('edges', key)][0])
         hptr = {key: put(('hrf', key), np.asarray(h, dtype=np.float64)) for key, h in hrfs.items()}
+        sptr = {key: put(('slots', key), c.slot_table(self.slot_width)) for key, c in conns.items()} \
+            if self.slot_width else {}
 
         insts = np.zeros(len(specs), dtype=_lib.INST_DTYPE)
         self._fed = []
@@ -438,6 +562,9 @@ class Batch:
             n, RL = m['n'], m['ring_len']
             d = insts[k]
             d['row_ptr'], d['edges'] = cptr[id(s.conn)]
+            if self.slot_width:
+                d['slots'] = sptr[id(s.conn)]
+                d['slot_width'] = self.slot_width
             V = self.lanes
             if V == 1:
                 d['ring'] = put(('ring', k), ring_from_reference(s.ring0, s.step0, RL))
