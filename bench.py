@@ -447,7 +447,7 @@ def main():
     batch = sw.build()
     batch.snapshot()
     n_steps = sw.n_steps
-    launches_per_step = int(np.ceil(n_steps / (args.chunk or n_steps))) + 1
+    launches_per_step = None   # the simulation launches of one step (Batch.run counts them) + the FC kernel
     nnz = sw._sim._conn.nnz
     st = torch.cuda.current_stream()
 
@@ -464,6 +464,7 @@ def main():
     for _ in range(args.warmup):
         one_step()
     torch.cuda.synchronize()
+    launches_per_step = batch.last_launches + 1
 
     sampler = ClockSampler(local)
     sampler.start()
@@ -520,6 +521,8 @@ def main():
     except OSError:
         pass
     peak = float(peaks.get('hbm_gbs', 6650.0))
+    peak_src = ('measured HBM copy bandwidth (of measured)' if 'hbm_gbs' in peaks
+                else 'the pool\'s earlier HBM measurement, 6650 GB/s (of fallback: no measured peaks file)')
     achieved = gather_bytes / t_kern / 1e9
     if rank == 0:
         line = {
@@ -542,9 +545,10 @@ def main():
                          'frac': achieved / peak,
                          'traffic': NCU_DRAM_BYTES_PER_INSTANCE_STEP * args.instances * n_steps,
                          'note': 'algorithmic gather bytes 4*ncvar*nnz per instance-step over the simulation '
-                                 'kernel time; peak = measured HBM copy bandwidth (of measured); traffic = ncu '
+                                 'kernel time; peak = %s; traffic = ncu '
                                  'DRAM bytes per launch, scaled from a 296-instance x 40 000-step capture; the '
-                                 'rings are staged in shared memory, so DRAM carries only staging and Bold'},
+                                 'rings are staged in shared memory, so DRAM carries only staging and Bold'
+                                 % peak_src},
             'gpu_launches': launches_per_step * args.steps,
             'kernel_ms_per_step': 1e3 * t_kern,
             'nonfinite_instances': int((status != 0).sum()),

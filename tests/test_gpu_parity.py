@@ -730,3 +730,31 @@ def test_projection_sweep_matches_simulator():
                         simulation_length=40.0).configure()
         (t, y), = sim.run()
         report('projection sweep instance %d vs Simulator' % i, res['projection'][0][i], y[..., 0], 1e-5)
+
+
+def test_wave_balanced_launches_equal_one_launch():
+    """A batch of one wave of resident CTAs plus a few instances runs as launches of exactly one wave each over
+    a cyclic instance order (inst_order); every instance's trajectory and Bold equal those of one launch over
+    all instances, bit for bit."""
+    import bench
+    b0 = bench.make_sweep(2, 500.0).configure().build()
+    R = b0.occupancy() * torch_sms()
+    assert R > 0
+    N = R + 37
+    runs = {}
+    for waves in (False, True):
+        s = bench.make_sweep(N, 500.0).configure()
+        b = s.build()
+        b.run(waves=waves)
+        if waves:
+            assert b.last_launches > 1 and b._wave_plan(5000) is not None
+        runs[waves] = (np.stack([b.state(i) for i in range(N)]), b.outputs_host(), b.status())
+    np.testing.assert_array_equal(runs[True][0], runs[False][0])
+    for o1, o0 in zip(runs[True][1], runs[False][1]):
+        np.testing.assert_array_equal(o1['bold'], o0['bold'])
+    assert (runs[True][2] == 0).all()
+
+
+def torch_sms():
+    import torch
+    return torch.cuda.get_device_properties(0).multi_processor_count

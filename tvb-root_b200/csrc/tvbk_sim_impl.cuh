@@ -797,7 +797,10 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     constexpr int NG = GatherTraits<CF, NCV>::NG;
     extern __shared__ __align__(16) float smem[];
 
-    tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x;
+    // this CTA's instance: the launch may take a subset of the batch through inst_order
+    const int b = L.inst_order != nullptr ? L.inst_order[blockIdx.x] : (int)blockIdx.x;
+    tvbk_inst* __restrict__ Ip = L.insts + b;
+    int32_t* const status = L.status + b;
     const int n = Ip->n;
     const int i = threadIdx.x;
     const bool act = i < n;
@@ -827,9 +830,9 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     Node<M, SCHEME, EXT> node;
     if (act) {
         const int e0 = Ip->row_ptr[i], e1 = Ip->row_ptr[i + 1];
-        if (MAXD > 0 && e1 - e0 > MAXD) atomicOr(L.status + blockIdx.x, TVBK_STATUS_DEGREE);
+        if (MAXD > 0 && e1 - e0 > MAXD) atomicOr(status, TVBK_STATUS_DEGREE);
         if (!EXT && (Ip->stim != nullptr || Ip->aff != nullptr || Ip->proj != nullptr))
-            atomicOr(L.status + blockIdx.x, TVBK_STATUS_UNSUPPORTED);
+            atomicOr(status, TVBK_STATUS_UNSUPPORTED);
         if constexpr (MAXD > 0) {
             if (Ip->slots != nullptr && Ip->slot_width == MAXD)
                 row.load_slots(Ip->slots, i, e0, e1);
@@ -964,7 +967,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         }
     }
     __syncthreads();
-    if (act) node.finish(L, Ip, i, n, L.status + blockIdx.x);
+    if (act) node.finish(L, Ip, i, n, status);
     if (SMEM && !SIGMA) stage_ring(Ip->ring, smem, ring_floats);
     if (i == 0) Ip->step = s_end;
 }
@@ -1122,6 +1125,12 @@ int launch_one(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
         if (e != cudaSuccess) return (int)e;
     }
     const int threads = ((L.max_n + 31) / 32) * 32;
+    if (L.occupancy != nullptr) {  // a query: resident CTAs per SM of this variant, no launch
+        int nb = 0;
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, smem_bytes);
+        *L.occupancy = nb;
+        return (int)e;
+    }
     kern<<<L.n_inst, threads, smem_bytes, st>>>(L);
     return (int)cudaGetLastError();
 }

@@ -116,6 +116,8 @@ class Launch(ctypes.Structure):
         ('cluster', ctypes.c_int32),
         ('cluster_edges', ctypes.c_int32),
         ('extras', ctypes.c_int32),
+        ('inst_order', ctypes.c_void_p),
+        ('occupancy', ctypes.c_void_p),
         ('max_steps', ctypes.c_int64),
         ('dt', ctypes.c_float),
     ]

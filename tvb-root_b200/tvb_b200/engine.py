@@ -692,17 +692,96 @@ class Batch:
         L.dt = self.dt
         return L
 
-    def run(self, n_steps=None, chunk=None, stream=None, graph=False):
+    def occupancy(self):
+        """Resident CTAs per SM of the row kernel variant this batch launches
+        (0 for the other kernels)."""
+        if self.lanes > 1 or self.cluster or self.edges_per_thread or self.prefetch == 2:
+            return 0
+        L = self.launch_struct(1)
+        occ = ctypes.c_int32(0)
+        L.occupancy = ctypes.addressof(occ)
+        st = torch.cuda.current_stream(self.device)
+        _lib.check(self.lib.tvbk_sim_run(ctypes.byref(L), ctypes.c_void_p(st.cuda_stream)))
+        return int(occ.value)
+
+    WAVE_MIN_CHUNK = 2000     # steps: a launch's ring stage-in / write-back stays negligible
+    WAVE_MAX_CHUNKS = 64
+
+    def _wave_plan(self, left):
+        """Round-robin windows of exactly one wave of resident CTAs, for a batch
+        of more instances than one wave that is not a whole number of waves
+        (one launch would leave its last wave partly empty): each instance runs
+        in C chunks and every launch takes the next R instances of the cyclic
+        instance order, so all launches but possibly the last are full waves.
+        Returns (R, C, chunk steps, launches) or None."""
+        specs = self.specs
+        if len({s.n_steps for s in specs}) != 1 or left <= 0 or self.device.type != 'cuda':
+            return None
+        key = ('wave_plan', left)
+        if getattr(self, '_wave_key', None) == key:
+            return self._wave_cached
+        self._wave_key, self._wave_cached = key, self._make_wave_plan(left)
+        return self._wave_cached
+
+    def _make_wave_plan(self, left):
+        specs = self.specs
+        occ = self.occupancy()
+        if occ <= 0:
+            return None
+        R = occ * torch.cuda.get_device_properties(self.device).multi_processor_count
+        N = len(specs)
+        if N <= R or N % R == 0:
+            return None
+        best = None
+        for C in range(2, self.WAVE_MAX_CHUNKS + 1):
+            chunk = -(-left // C)
+            if chunk < self.WAVE_MIN_CHUNK:
+                break
+            launches = -(-N * C // R)
+            eff = N * C / (launches * R)
+            if best is None or eff > best[0] + 1e-9:
+                best = (eff, C, chunk, launches)
+            if eff >= 0.995:
+                break
+        one = N / (-(-N // R) * R)          # the fill of one launch over all instances
+        if best is None or best[0] <= one:
+            return None
+        return R, best[1], best[2], best[3]
+
+    def run(self, n_steps=None, chunk=None, stream=None, graph=False, waves=True):
         """Advance every instance by up to n_steps (default: to its end) in
         launches of at most `chunk` steps.
 
         graph=True: the chunk launches are recorded once into a CUDA graph of
         up to `graph_launches` launches (the kernel reads each instance's step
         from its device descriptor, so replaying the same launches continues
-        the run) and the graph is replayed; a remainder runs eagerly."""
+        the run) and the graph is replayed; a remainder runs eagerly.
+
+        waves=True with no chunk given: a batch of more instances than fit at
+        once, not a whole number of waves, runs as launches of exactly one wave
+        each over a cyclic instance order (see _wave_plan); the same steps,
+        without the last wave's idle SMs."""
         left = self.max_total - self.steps_done if n_steps is None else int(n_steps)
-        chunk = left if chunk is None else int(chunk)
         st = torch.cuda.current_stream(self.device) if stream is None else stream
+        plan = self._wave_plan(left) if (waves and chunk is None and not graph) else None
+        if plan is not None:
+            R, C, wchunk, launches = plan
+            N = len(self.specs)
+            if getattr(self, '_order_dev', None) is None:
+                with torch.cuda.stream(st):
+                    self._order_dev = torch.as_tensor(np.tile(np.arange(N, dtype=np.int32), 2), device=self.device)
+            base = self._order_dev.data_ptr()
+            for j in range(launches):
+                start = (j * R) % N
+                L = self.launch_struct(wchunk)
+                L.inst_order = base + 4 * start
+                L.n_inst = min(R, N * C - j * R)
+                _lib.check(self.lib.tvbk_sim_run(ctypes.byref(L), ctypes.c_void_p(st.cuda_stream)))
+            self.steps_done += left
+            self.last_launches = launches
+            return
+        chunk = left if chunk is None else int(chunk)
+        self.last_launches = 0
         if graph and chunk > 0 and left >= 2 * chunk:
             reps = left // chunk
             g = self._chunk_graph(chunk, min(reps, self.graph_launches), st)
@@ -713,12 +792,14 @@ class Batch:
             done = (reps // per) * per * chunk
             left -= done
             self.steps_done += done
+            self.last_launches += (reps // per) * per
         while left > 0:
             k = min(chunk, left)
             L = self.launch_struct(k)
             _lib.check(self.lib.tvbk_sim_run(ctypes.byref(L), ctypes.c_void_p(st.cuda_stream)))
             left -= k
             self.steps_done += k
+            self.last_launches += 1
 
     graph_launches = 64
 
