@@ -758,3 +758,22 @@ def test_wave_balanced_launches_equal_one_launch():
 def torch_sms():
     import torch
     return torch.cuda.get_device_properties(0).multi_processor_count
+
+
+def test_shared_history_upload_and_stacked_outputs():
+    """Instances that share an initial history get it from one upload and device copies (each ring equal to
+    its own conversion of the history), and the stacked Bold view equals the per-instance outputs."""
+    import torch
+    import bench
+    from tvb_b200.engine import ring_from_reference
+    sw = bench.make_sweep(5, 4200.0).configure()
+    b = sw.build()
+    s0 = b.specs[0]
+    want = ring_from_reference(s0.ring0, s0.step0, b.meta[0]['ring_len'])
+    for k in range(5):
+        np.testing.assert_array_equal(np.asarray(b.ring(k)).reshape(want.shape), want)
+    assert b.h2d_bytes < b.init.size
+    sw.run_device()
+    st = b.stacked_output('bold', torch.float64)
+    for k in range(5):
+        torch.testing.assert_close(st[k], b.outputs_device(k)['bold'], rtol=0, atol=0)

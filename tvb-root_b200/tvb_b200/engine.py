@@ -27,6 +27,16 @@ def _aligned(x):
     return (x + ALIGN - 1) // ALIGN * ALIGN
 
 
+def _array_key(a):
+    """Identity of an array's contents by its memory (views of one buffer with
+    the same layout are the same input), else of the object."""
+    if isinstance(a, np.ndarray):
+        return ('np', a.__array_interface__['data'][0], a.shape, a.strides, a.dtype.str)
+    if isinstance(a, torch.Tensor):
+        return ('torch', a.data_ptr(), tuple(a.shape), tuple(a.stride()), str(a.dtype))
+    return ('obj', id(a))
+
+
 class _Arena:
     """Byte offsets of named regions in one allocation."""
 
@@ -452,6 +462,17 @@ class Batch:
         """Arena layout and per-instance metadata (no device memory)."""
         specs, nvoi = self.specs, self.nvoi
         init, zero, outa = _Arena(), _Arena(), _Arena()
+        # the rings first, one block: instances that start from the same history (a sweep) upload it once
+        # and it is copied on the device
+        self._ring_src = {}
+        if self.lanes == 1:
+            first = {}
+            for k, s in enumerate(specs):
+                RL = self._ring_len(s)
+                init.add(('ring', k), RL * s.conn.n * self.ncvar * 4)
+                key = (_array_key(s.ring0), s.step0, RL)
+                self._ring_src[k] = first.setdefault(key, k)
+        self._ring_block = init.size
         conns = {}
         for s in specs:
             if id(s.conn) not in conns:
@@ -468,7 +489,7 @@ class Batch:
             RL = self._ring_len(s)
             m = dict(n=n, ring_len=RL)
             V = self.lanes
-            if k % V == 0:
+            if V > 1 and k % V == 0:
                 init.add(('ring', k), V * RL * n * self.ncvar * 4)
             if self.sigma and not self.ring_in_smem:
                 zero.add(('pre_ring', k), RL * n * 4)
@@ -530,12 +551,19 @@ class Batch:
         self.out_buf = torch.zeros(max(outa.size, 1), dtype=torch.uint8, device=dev)
         ib, zb, ob = self.init_buf.data_ptr(), self.zero_buf.data_ptr(), self.out_buf.data_ptr()
 
-        stage = np.zeros(max(init.size, 1), dtype=np.uint8)
+        # host staging of everything after the ring block; the rings themselves are uploaded once per
+        # distinct history
+        R0 = self._ring_block
+        stage = np.zeros(max(init.size - R0, 1), dtype=np.uint8)
+        ring_up = {}
 
         def put(key, arr):
             off, nb = init.regions[key]
             a = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
-            stage[off:off + a.size] = a
+            if off < R0:
+                ring_up[key] = a
+            else:
+                stage[off - R0:off - R0 + a.size] = a
             return ib + off
 
         def zaddr(key):
@@ -567,7 +595,11 @@ class Batch:
                 d['slot_width'] = self.slot_width
             V = self.lanes
             if V == 1:
-                d['ring'] = put(('ring', k), ring_from_reference(s.ring0, s.step0, RL))
+                src = self._ring_src[k]
+                if src == k:
+                    d['ring'] = put(('ring', k), ring_from_reference(s.ring0, s.step0, RL))
+                else:
+                    d['ring'] = ib + init.regions[('ring', k)][0]
             elif k % V == 0:
                 group = [ring_from_reference(specs[k + v].ring0, specs[k + v].step0, RL) for v in range(V)]
                 d['ring'] = put(('ring', k), np.stack(group, axis=-1))  # [RL][n][ncvar][V]
@@ -641,9 +673,45 @@ class Batch:
         self.insts_host = insts
         self.insts_ptr = put(('insts',), insts)
         self.status_ptr = zaddr(('status',))
-        self.init_buf.copy_(torch.from_numpy(stage))
+        if init.size > R0:
+            self.init_buf[R0:init.size].copy_(torch.from_numpy(stage[:init.size - R0]))
+        self._upload_rings(ring_up)
         self.steps_done = 0
         self.max_total = max(s.n_steps for s in specs)
+
+    def _upload_rings(self, ring_up):
+        """Host-to-device copy of each distinct initial ring, then device copies
+        to the instances that share it (one broadcast copy when the regions
+        are evenly spaced)."""
+        self._h2d_ring_bytes = 0
+        groups = {}
+        for k, src in self._ring_src.items():
+            groups.setdefault(src, []).append(k)
+        if groups and len(groups) == len(self._ring_src):
+            # every instance has its own history: one staged copy of the whole ring block
+            R0 = self._ring_block
+            stage = np.zeros(R0, dtype=np.uint8)
+            for (_, k), a in ring_up.items():
+                off = self.init.regions[('ring', k)][0]
+                stage[off:off + a.size] = a
+            self.init_buf[:R0].copy_(torch.from_numpy(stage))
+            self._h2d_ring_bytes = R0
+            return
+        for src, ks in groups.items():
+            off, nb = self.init.regions[('ring', src)]
+            a = ring_up[('ring', src)]
+            self.init_buf[off:off + nb].copy_(torch.from_numpy(a))
+            self._h2d_ring_bytes += nb
+            dst = [self.init.regions[('ring', k)][0] for k in ks if k != src]
+            if not dst:
+                continue
+            steps = np.diff(dst)
+            if len(dst) > 1 and (steps == steps[0]).all() and steps[0] >= nb:
+                view = self.init_buf[dst[0]:dst[-1] + nb].as_strided((len(dst), nb), (int(steps[0]), 1))
+                view.copy_(self.init_buf[off:off + nb].expand(len(dst), nb))
+            else:
+                for d in dst:
+                    self.init_buf[d:d + nb].copy_(self.init_buf[off:off + nb])
 
     # ------------------------------------------------------------------ reset
     def snapshot(self):
@@ -660,7 +728,8 @@ class Batch:
 
     @property
     def h2d_bytes(self):
-        return self.init.size + sum(int(f.numel()) * 4 for f in self._fed)
+        return (self.init.size - self._ring_block + getattr(self, '_h2d_ring_bytes', 0)
+                + sum(int(f.numel()) * 4 for f in self._fed))
 
     @property
     def d2h_bytes(self):
@@ -855,8 +924,32 @@ class Batch:
         return out
 
     def outputs_host(self):
-        """All outputs of all instances as numpy arrays, from one device-to-host copy."""
-        return self.outputs_from_bytes(self.out_buf.cpu().numpy())
+        """All outputs of all instances as numpy arrays, from one device-to-host
+        copy into pinned memory."""
+        host = torch.empty(self.out_buf.numel(), dtype=torch.uint8, pin_memory=True)
+        host.copy_(self.out_buf, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return self.outputs_from_bytes(host.numpy())
+
+    def stacked_output(self, key, dtype=torch.float64):
+        """Device view (I, T, nvoi, n) of one output of every instance without a
+        copy when the instances' regions are evenly spaced and equally long,
+        else a stacked copy."""
+        rows = key + '_rows'
+        metas = self.meta
+        if not all(rows in m for m in metas) or len({m[rows] for m in metas}) != 1 \
+                or len({m['n'] for m in metas}) != 1:
+            return torch.stack([self.outputs_device(i)[key] for i in range(len(metas))])
+        T, n = metas[0][rows], metas[0]['n']
+        nv = self.ncvar if key == 'aff' else self.nvoi
+        item = torch.empty((), dtype=dtype).element_size()
+        offs = np.array([self.out.regions[(key, i)][0] for i in range(len(metas))])
+        steps = np.diff(offs)
+        if len(offs) > 1 and not ((steps == steps[0]).all() and steps[0] % item == 0 and offs[0] % item == 0):
+            return torch.stack([self.outputs_device(i)[key] for i in range(len(metas))])
+        stride = int(steps[0]) // item if len(offs) > 1 else T * nv * n
+        base = self.out_buf[:self.out_buf.numel() // item * item].view(dtype)
+        return base.as_strided((len(metas), T, nv, n), (stride, nv * n, n, 1), int(offs[0]) // item)
 
     def outputs_from_bytes(self, host):
         """Per-instance output arrays from a host copy (uint8 array) of the output arena."""

@@ -193,7 +193,7 @@ class ParameterSweep:
 
     def bold_device(self, voi=0):
         """(I, T, n) float64 device tensor of the Bold series of one observed variable."""
-        return torch.stack([self.batch.outputs_device(i)['bold'][:, voi, :] for i in range(self.n_instances)])
+        return self.batch.stacked_output('bold', torch.float64)[:, :, voi, :]
 
     def fc_device(self, voi=0):
         """Per-instance functional connectivity (I, n, n) float64 on the device."""
