@@ -78,7 +78,9 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-template <class M, int CF, int SCHEME, int MAXE, bool PIPE>
+// EXT = false: built without the region stimulus and the projection stream
+// (launch.extras == 0), whose per-thread state would otherwise spill here.
+template <class M, int CF, int SCHEME, int MAXE, bool PIPE, bool EXT = true>
 __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const tvbk_launch L) {
     constexpr int NCV = M::NCV;
     constexpr int NACC = (CF == CF_SIGMOIDAL_JR) ? 1 : NCV;
@@ -123,11 +125,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const t
     const int G0 = PIPE ? U : 0;                   // first gather warp
     const int G = PIPE ? W - U : W;                // gather warps
     const bool upd = tid < nr;
-    Node<M, SCHEME> node;
+    Node<M, SCHEME, EXT> node;
     if (upd) {
         node.init(L, Ip, r0 + tid, n, s0);
         if (Ip->row_ptr[r0 + tid + 1] - Ip->row_ptr[r0 + tid] > 32 * MAXE) atomicOr(status, TVBK_STATUS_DEGREE);
-        if (Ip->aff != nullptr) atomicOr(status, TVBK_STATUS_UNSUPPORTED);
+        if (Ip->aff != nullptr || (!EXT && (Ip->stim != nullptr || Ip->proj != nullptr)))
+            atomicOr(status, TVBK_STATUS_UNSUPPORTED);
     }
     float* __restrict__ raw = Ip->ring;
     // gather ring: the raw ring, or for SigmoidalJansenRit the pre-applied sigmoid values, recomputed from
@@ -226,9 +229,9 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const t
     if (rank == 0 && tid == 0) Ip->step = s_end;
 }
 
-template <class M, int CF, int SCHEME, int MAXE, bool PIPE>
+template <class M, int CF, int SCHEME, int MAXE, bool PIPE, bool EXT>
 int launch_cluster_t(const tvbk_launch& L, cudaStream_t st) {
-    auto kern = sim_kernel_cluster<M, CF, SCHEME, MAXE, PIPE>;
+    auto kern = sim_kernel_cluster<M, CF, SCHEME, MAXE, PIPE, EXT>;
     constexpr int NACC = (CF == CF_SIGMOIDAL_JR) ? 1 : M::NCV;
     const int C = L.cluster;
     const int R = cluster_rows(L.max_n, C);
@@ -256,19 +259,23 @@ int launch_cluster_t(const tvbk_launch& L, cudaStream_t st) {
     return (int)e;
 }
 
-template <class M, int CF, int SCHEME, bool PIPE>
+template <class M, int CF, int SCHEME, bool PIPE, bool EXT>
 int launch_cluster_p(const tvbk_launch& L, cudaStream_t st) {
-    if (L.max_degree <= 64) return launch_cluster_t<M, CF, SCHEME, 2, PIPE>(L, st);
-    if (L.max_degree <= 128) return launch_cluster_t<M, CF, SCHEME, 4, PIPE>(L, st);
-    if (L.max_degree <= 256) return launch_cluster_t<M, CF, SCHEME, 8, PIPE>(L, st);
-    if (L.max_degree <= 1024) return launch_cluster_t<M, CF, SCHEME, 32, PIPE>(L, st);
+    if (L.max_degree <= 64) return launch_cluster_t<M, CF, SCHEME, 2, PIPE, EXT>(L, st);
+    if (L.max_degree <= 128) return launch_cluster_t<M, CF, SCHEME, 4, PIPE, EXT>(L, st);
+    if (L.max_degree <= 256) return launch_cluster_t<M, CF, SCHEME, 8, PIPE, EXT>(L, st);
+    if (L.max_degree <= 1024) return launch_cluster_t<M, CF, SCHEME, 32, PIPE, EXT>(L, st);
     return -1;
 }
 
 template <class M, int CF, int SCHEME>
 int launch_cluster(const tvbk_launch& L, cudaStream_t st) {
-    if (L.prefetch) return launch_cluster_p<M, CF, SCHEME, true>(L, st);
-    return launch_cluster_p<M, CF, SCHEME, false>(L, st);
+    if (L.extras == 0) {
+        if (L.prefetch) return launch_cluster_p<M, CF, SCHEME, true, false>(L, st);
+        return launch_cluster_p<M, CF, SCHEME, false, false>(L, st);
+    }
+    if (L.prefetch) return launch_cluster_p<M, CF, SCHEME, true, true>(L, st);
+    return launch_cluster_p<M, CF, SCHEME, false, true>(L, st);
 }
 
 }  // namespace tvbk
