@@ -583,12 +583,13 @@ class Batch:
         sptr = {key: put(('slots', key), c.slot_table(self.slot_width)) for key, c in conns.items()} \
             if self.slot_width else {}
 
-        insts = np.zeros(len(specs), dtype=_lib.INST_DTYPE)
+        # descriptor fields per instance as dicts, written into the structured array column by column
+        recs = [dict() for _ in specs]
         self._fed = []
         for k, s in enumerate(specs):
             m = self.meta[k]
             n, RL = m['n'], m['ring_len']
-            d = insts[k]
+            d = recs[k]
             d['row_ptr'], d['edges'] = cptr[id(s.conn)]
             if self.slot_width:
                 d['slots'] = sptr[id(s.conn)]
@@ -604,7 +605,7 @@ class Batch:
                 group = [ring_from_reference(specs[k + v].ring0, specs[k + v].step0, RL) for v in range(V)]
                 d['ring'] = put(('ring', k), np.stack(group, axis=-1))  # [RL][n][ncvar][V]
             else:
-                d['ring'] = insts[k - k % V]['ring']
+                d['ring'] = recs[k - k % V]['ring']
             d['pre_ring'] = zaddr(('pre_ring', k))
             d['state'] = put(('state', k), np.asarray(s.state0, dtype=np.float32))
             params = np.asarray(s.params, dtype=np.float32)
@@ -670,6 +671,11 @@ class Batch:
             d['cfun'] = cf
             d['seed'] = s.seed & 0xFFFFFFFF
             d['stream'] = s.stream & 0xFFFFFFFF
+        insts = np.zeros(len(specs), dtype=_lib.INST_DTYPE)
+        for name in _lib.INST_DTYPE.names:
+            if any(name in r for r in recs):
+                blank = np.zeros((), dtype=_lib.INST_DTYPE[name])
+                insts[name] = [r.get(name, blank) for r in recs]
         self.insts_host = insts
         self.insts_ptr = put(('insts',), insts)
         self.status_ptr = zaddr(('status',))
