@@ -162,6 +162,8 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
     L2.max_n = inst->n;
     L2.max_ring_len = inst->ring_len;
     L2.max_steps = inst->step_end - inst->step;
+    L2.inst_order = nullptr;  // one instance, the staged descriptor
+    L2.occupancy = nullptr;   // always a launch
     const int rc = tvbk_sim_run(&L2, stream);
     if (rc != TVBK_OK) return rc;  // tvbk_sim_run has set the message
     if (status_out) {
