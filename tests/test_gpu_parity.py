@@ -777,3 +777,26 @@ def test_shared_history_upload_and_stacked_outputs():
     st = b.stacked_output('bold', torch.float64)
     for k in range(5):
         torch.testing.assert_close(st[k], b.outputs_device(k)['bold'], rtol=0, atol=0)
+
+
+def test_rawvoi_and_progress_logger_on_the_device():
+    """RawVoi is the Raw stream's chosen variables; ProgressLogger returns no samples, in run() and in the
+    step generator."""
+    from tvb_b200 import coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.simulator import Simulator
+    w, L = synthetic.connectome(16, 0.5, 5.0, 30.0, seed=1)
+
+    def make():
+        np.random.seed(4)
+        return Simulator(model=models.JansenRit(), connectivity=Connectivity(w, L, speed=3.0),
+                         coupling=coupling.SigmoidalJansenRit(), integrator=integrators.HeunDeterministic(dt=0.1),
+                         monitors=[monitors.RawVoi(variables_of_interest=[1, 3]), monitors.Raw(),
+                                   monitors.ProgressLogger(period=2.0)], simulation_length=5.0).configure()
+    (t1, y1), (t0, y0), (tp, yp) = make().run()
+    np.testing.assert_array_equal(t1, t0)
+    np.testing.assert_array_equal(y1, y0[:, [1, 3]])
+    assert tp.size == 0 and yp.size == 0
+    rows = list(make()())
+    assert len(rows) == 50 and all(r[2] is None for r in rows)
+    np.testing.assert_array_equal(np.stack([r[0][1] for r in rows]), y1)

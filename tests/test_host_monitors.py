@@ -97,3 +97,19 @@ def test_projection_finish_noise_and_reference():
     want = y + np.stack([np.sqrt(0.1) * rs.normal(size=(16, 1)).T for _ in range(5)])
     want = want - want.mean(axis=2, keepdims=True)
     np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+
+
+def test_rawvoi_and_progress_logger_configuration():
+    """RawVoi keeps the chosen variables of interest (monitors.py:193-211); ProgressLogger records nothing and
+    logs every int(period / dt) steps (monitors.py:1005-1026)."""
+    from tvb_b200 import coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.simulator import Simulator
+    w, L = synthetic.connectome(10, 0.5, 5.0, 30.0, seed=1)
+    mons = [monitors.RawVoi(variables_of_interest=[1, 3]), monitors.Raw(), monitors.ProgressLogger(period=2.0)]
+    sim = Simulator(model=models.JansenRit(), connectivity=Connectivity(w, L, speed=3.0),
+                    coupling=coupling.SigmoidalJansenRit(), integrator=integrators.HeunDeterministic(dt=0.1),
+                    monitors=mons, simulation_length=5.0).configure()
+    assert list(mons[0].voi) == [1, 3] and mons[0].istep == 1
+    assert len(mons[1].voi) == len(sim.model.variables_of_interest)
+    assert mons[2].istep == 20

@@ -60,6 +60,33 @@ class Raw(Monitor):
         return steps * self.dt
 
 
+class RawVoi(Raw):
+    """Every step, the chosen variables of interest (monitors.py:193-211)."""
+
+    def _config_vois(self, sim):
+        Monitor._config_vois(self, sim)
+
+
+class ProgressLogger(Monitor):
+    """Logs the step and time every int(period / dt) steps from the first
+    step it sees and records nothing (monitors.py:1005-1026)."""
+    default_period = 1000.0
+
+    def _config_time(self, sim):
+        self.dt = sim.integrator.dt
+        self.istep = max(int(self.period / self.dt), 1)
+        self._first = None
+
+    def log_steps(self, steps):
+        import logging
+        log = logging.getLogger(__name__)
+        for s in np.asarray(steps):
+            if self._first is None:
+                self._first = int(s)
+            if (int(s) - self._first) % self.istep == 0:
+                log.info('step %d time %.4f s', int(s), int(s) * self.dt / 1e3)
+
+
 class TemporalAverage(Monitor):
     """Mean over each period, stamped at its middle (monitors.py:363-391)."""
 
@@ -222,8 +249,8 @@ class AfferentCouplingTemporalAverage(AfferentCoupling):
         return samples, acc
 
 
-MONITORS = {c.__name__: c for c in (Raw, TemporalAverage, Bold, SubSample, GlobalAverage, SpatialAverage,
-                                    AfferentCoupling, AfferentCouplingTemporalAverage)}
+MONITORS = {c.__name__: c for c in (Raw, RawVoi, ProgressLogger, TemporalAverage, Bold, SubSample, GlobalAverage,
+                                    SpatialAverage, AfferentCoupling, AfferentCouplingTemporalAverage)}
 
 
 def _array(obj, attr):

@@ -86,6 +86,10 @@ def adopt_monitor(mon):
         voi = None
     if name == 'Raw':
         return monitors_mod.Raw()
+    if name == 'RawVoi':
+        return monitors_mod.RawVoi(variables_of_interest=voi)
+    if name == 'ProgressLogger':
+        return monitors_mod.ProgressLogger(period=mon.period)
     if name == 'TemporalAverage':
         return monitors_mod.TemporalAverage(period=mon.period, variables_of_interest=voi)
     if name in ('SubSample', 'GlobalAverage', 'AfferentCouplingTemporalAverage'):
@@ -371,6 +375,10 @@ class Simulator:
         res = []
         steps = np.arange(s0 + 1, s0 + n_steps + 1)
         for k, m in enumerate(self.monitors):
+            if isinstance(m, monitors_mod.ProgressLogger):
+                m.log_steps(steps)
+                res.append((np.array([]), np.array([])))
+                continue
             if isinstance(m, monitors_mod.Raw):
                 t, y = m.times(steps.astype(np.float64)), out['raw'][:, m.voi]
             elif isinstance(m, monitors_mod.TemporalAverage):
@@ -424,7 +432,8 @@ class Simulator:
             sample_steps = []
             for m in self.monitors:
                 steps = np.arange(s0 + 1, s0 + k + 1)
-                sample_steps.append(set(steps[steps % m.istep == 0].tolist()))
+                sample_steps.append(set() if isinstance(m, monitors_mod.ProgressLogger)
+                                    else set(steps[steps % m.istep == 0].tolist()))
             for step in range(s0 + 1, s0 + k + 1):
                 row = []
                 for j, m in enumerate(self.monitors):
@@ -585,6 +594,7 @@ class Simulator:
             self.integrator.noise.random_stream.set_state(random_state)
         if n_steps is None:
             n_steps = int(math.ceil(self.simulation_length / self.integrator.dt))
+        self._prepare_stimulus()
         left = int(n_steps)
         parts = [[] for _ in self.monitors]
         while left > 0:
