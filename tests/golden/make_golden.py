@@ -616,6 +616,20 @@ def case_stimulus(R):
             out['%s_m%d_t' % (name, k)] = t
         if rec is not None:
             out[name + '_noise_sha256'] = rec.h.hexdigest()
+    # two calls of 30 ms: the reference evaluates the temporal pattern again at each call, from its start
+    def build2():
+        conn = make_conn(R, w, L, speed)
+        stim = P.StimuliRegion(temporal=E.PulseTrain(parameters={'T': 12.0, 'tau': 4.0, 'amp': 2.0, 'onset': 5.0}),
+                               connectivity=conn, weight=weight)
+        return R['simulator'].Simulator(model=M.Generic2dOscillator(), connectivity=conn,
+                                        coupling=C.Linear(a=np.array([0.0152])),
+                                        integrator=I.HeunDeterministic(dt=0.1), monitors=[R['monitors'].Raw()],
+                                        simulation_length=30.0, stimulus=stim)
+    sim, cfg, res, _, _ = run_sim(R, build2, 30.0, False, ic_seed=301)
+    (t1, y1), = res
+    (t2, y2), = sim.run(simulation_length=30.0)
+    out.update(g2d_2x_buffer0=cfg['buffer0'], g2d_2x_state0=cfg['state0'], g2d_2x_t=np.concatenate([t1, t2]),
+               g2d_2x_raw=np.concatenate([y1, y2])[..., 0])
     save('stimulus_40', **out)
 
 

@@ -800,3 +800,25 @@ def test_rawvoi_and_progress_logger_on_the_device():
     rows = list(make()())
     assert len(rows) == 50 and all(r[2] is None for r in rows)
     np.testing.assert_array_equal(np.stack([r[0][1] for r in rows]), y1)
+
+
+def test_region_stimulus_across_two_run_calls():
+    """A second run() call evaluates the stimulus' temporal pattern again from its start (simulator.py:290-306),
+    as the reference does: two 30 ms calls against the reference's two calls."""
+    from tvb_b200 import coupling, equations, integrators, models, monitors
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.patterns import StimuliRegion
+    from tvb_b200.simulator import Simulator
+    fx = G.load('stimulus_40')
+    conn = Connectivity(fx['weights'], fx['tract_lengths'], speed=float(fx['speed']))
+    stim = StimuliRegion(temporal=equations.PulseTrain({'T': 12.0, 'tau': 4.0, 'amp': 2.0, 'onset': 5.0}),
+                         weight=fx['stim_weight'])
+    np.random.seed(301)
+    sim = Simulator(model=models.Generic2dOscillator(), connectivity=conn, coupling=coupling.Linear(a=0.0152),
+                    integrator=integrators.HeunDeterministic(dt=0.1), monitors=[monitors.Raw()],
+                    simulation_length=30.0, stimulus=stim).configure()
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx['g2d_2x_buffer0'])
+    (t1, y1), = sim.run()
+    (t2, y2), = sim.run(simulation_length=30.0)
+    np.testing.assert_allclose(np.concatenate([t1, t2]), fx['g2d_2x_t'], rtol=0, atol=1e-12)
+    report('stimulus two calls vs reference', np.concatenate([y1, y2])[..., 0], fx['g2d_2x_raw'], 1e-4)
