@@ -473,8 +473,8 @@ struct Node {
                 nz[k] = STOCH ? sig[k] * z[k] : 0.0f;
                 if constexpr (STOCH)
                     inter[k] = add_dt_st(x[k] + dt * m0[k] + nz[k], k);
-                else
-                    inter[k] = x[k] + dt * with_st(m0[k], k);
+                else  // + nz (0 here): the form of the stochastic predictor; it also schedules better
+                    inter[k] = x[k] + dt * with_st(m0[k], k) + nz[k];
             }
             M::bound(inter);
             float m1[NSV];
