@@ -822,3 +822,27 @@ def test_region_stimulus_across_two_run_calls():
     (t2, y2), = sim.run(simulation_length=30.0)
     np.testing.assert_allclose(np.concatenate([t1, t2]), fx['g2d_2x_t'], rtol=0, atol=1e-12)
     report('stimulus two calls vs reference', np.concatenate([y1, y2])[..., 0], fx['g2d_2x_raw'], 1e-4)
+
+
+@pytest.mark.parametrize('case', ['no_edges', 'zero_delays', 'one_region'])
+def test_edge_case_connectomes_vs_oracle(case):
+    """Connectomes at the edges of the layout: no non-zero weight (nnz = 0), every delay zero (horizon 1, a
+    ring of 2 slots, a barrier every step) and a single region, against the oracle from the same history."""
+    from tvb_b200 import coupling, integrators, models, monitors
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.simulator import Simulator
+    rng = np.random.default_rng(7)
+    n = 1 if case == 'one_region' else 40
+    w = np.zeros((n, n)) if case != 'zero_delays' else rng.uniform(0, 1, (n, n))
+    np.fill_diagonal(w, 0)
+    L = np.zeros((n, n)) if case != 'no_edges' else rng.uniform(5, 50, (n, n))
+    np.random.seed(9)
+    sim = Simulator(model=models.Generic2dOscillator(), connectivity=Connectivity(w, L, speed=3.0),
+                    coupling=coupling.Linear(a=0.05), integrator=integrators.HeunDeterministic(dt=0.1),
+                    monitors=[monitors.Raw()], simulation_length=20.0).configure()
+    buf0, st0 = sim.history_buffer[..., 0].copy(), sim.current_state[..., 0].copy()
+    (t, y), = sim.run()
+    out, _ = O.simulate('Generic2dOscillator', {}, w, L, 3.0, 0.1, 'Linear', {'a': 0.05}, 'HeunDeterministic', 200,
+                        [O.Monitor('Raw')], buf0, st0, 0)
+    assert y.shape == (200, 1, n, 1)
+    report('edge case %s vs oracle' % case, y[..., 0], out[0][1], 1e-4)
