@@ -288,17 +288,18 @@ def box_muller(u1, u2):
 
 def philox_normals(seed, stream, steps, nintvar, n):
     """Standard normals of the device noise stream for the given absolute steps:
-    block = Philox(key=(seed, stream), counter=(step >> 2, node, svar, 0)); the
-    pairs (x0, x1) and (x2, x3) give the normals of steps 4k..4k+1 and 4k+2..4k+3.
+    block = Philox(key=(seed, stream), counter=((step - 1) >> 2, node, svar, 0));
+    the pairs (x0, x1) and (x2, x3) give the normals of steps 4k+1..4k+2 and
+    4k+3..4k+4.
     Returns (len(steps), nintvar, n) float64."""
     steps = np.asarray(steps, dtype=np.int64)
-    blk = (steps >> 2).astype(np.uint32)[:, None, None]
+    blk = ((steps - 1) >> 2).astype(np.uint32)[:, None, None]
     node = np.arange(n, dtype=np.uint32)[None, None, :]
     sv = np.arange(nintvar, dtype=np.uint32)[None, :, None]
     x = philox4x32_10(blk, node, sv, np.uint32(0), np.uint32(seed & 0xFFFFFFFF), np.uint32(stream & 0xFFFFFFFF))
     za, zb = box_muller(uniform_open(x[0]), uniform_open(x[1]))
     zc, zd = box_muller(uniform_open(x[2]), uniform_open(x[3]))
-    sel = (steps & 3)[:, None, None]
+    sel = ((steps - 1) & 3)[:, None, None]
     return np.where(sel == 0, za, np.where(sel == 1, zb, np.where(sel == 2, zc, zd)))
 
 

@@ -7,11 +7,13 @@
 // a Box-Muller transform turns each pair into two normals.
 //
 // Stream layout (mirrored by the CPU oracle): the normal of (step s, region i,
-// state variable k) is element s & 3 of the 4 normals from
-// Philox(key = (seed, stream), counter = (s >> 2, i, k, 0)), the pairs
-// (x0, x1) and (x2, x3) giving steps 4q..4q+1 and 4q+2..4q+3.  The stream is
-// keyed by instance, not by batch slot, so a simulation draws the same noise
-// alone or batched with others.
+// state variable k) is element (s - 1) & 3 of the 4 normals from
+// Philox(key = (seed, stream), counter = ((s - 1) >> 2, i, k, 0)), the pairs
+// (x0, x1) and (x2, x3) giving steps 4q+1..4q+2 and 4q+3..4q+4.  Blocks end on
+// steps that are multiples of 4, where monitor samples with periods in
+// multiples of 4 steps fall (the 4 ms Bold stock, a TR).  The stream is keyed
+// by instance, not by batch slot, so a simulation draws the same noise alone
+// or batched with others.
 #pragma once
 #include <cstdint>
 
@@ -69,10 +71,14 @@ __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, fl
     z1 = -r * s;
 }
 
-// The 4 normals of block (s >> 2) for region i, state variable k.
+// Block of step s (>= 1): steps 4q+1 .. 4q+4 share block q = (s - 1) >> 2.
+__device__ __forceinline__ int64_t philox_block_of(int64_t step) { return (step - 1) >> 2; }
+__device__ __forceinline__ int philox_lane_of(int64_t step) { return (int)((step - 1) & 3); }
+
+// The 4 normals of the block of step s for region i, state variable k.
 __device__ __forceinline__ void philox_normals4(uint32_t seed, uint32_t stream, int64_t step, int i, int k,
                                                 float z[4]) {
-    const Philox4 r = philox4x32_10((uint32_t)(step >> 2), (uint32_t)i, (uint32_t)k, 0u, seed, stream);
+    const Philox4 r = philox4x32_10((uint32_t)philox_block_of(step), (uint32_t)i, (uint32_t)k, 0u, seed, stream);
     box_muller(r.x[0], r.x[1], z[0], z[1]);
     box_muller(r.x[2], r.x[3], z[2], z[3]);
 }

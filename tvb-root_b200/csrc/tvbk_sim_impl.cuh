@@ -35,9 +35,9 @@ struct SchemeTraits {
     static constexpr bool stoch = (SCHEME == TVBK_SCHEME_EULER_STOCH || SCHEME == TVBK_SCHEME_HEUN_STOCH);
 };
 
-// True at the first step of a launch and at every step s with s & 3 == 0:
+// True at the first step of a launch and at every step s with (s - 1) & 3 == 0:
 // where a new block of four Philox normals starts.
-#define STOCH_BLOCK_START(ks) ((ks) == 0 || ((s0 + 1 + (ks)) & 3) == 0)
+#define STOCH_BLOCK_START(ks) ((ks) == 0 || ((s0 + (ks)) & 3) == 0)
 
 // Per-edge pre() forms of the couplings whose pre / post are chosen at run
 // time (CF_GENERIC kernels): HyperbolicTangent a (1 + tanh((b x_j - midpoint)
@@ -425,7 +425,7 @@ struct Node {
         }
     }
 
-    // Philox normals of the 4-step block of step s (steps 4q .. 4q+3, q = s >> 2).
+    // Philox normals of the 4-step block of step s (steps 4q+1 .. 4q+4, q = (s - 1) >> 2).
     __device__ __forceinline__ void noise_block(const tvbk_launch& L, int i, int64_t s) {
         if constexpr (STOCH) {
             if (L.noise == TVBK_NOISE_PHILOX) {
@@ -520,7 +520,7 @@ struct Node {
                 for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
                 fed_p += (size_t)NINT * n;
             } else {
-                const int r = (int)((s0 + 1 + ks) & 3);
+                const int r = philox_lane_of(s0 + 1 + ks);
 #pragma unroll
                 for (int k = 0; k < NINT; ++k)
                     z[k] = (r == 0) ? zc[k][0] : (r == 1) ? zc[k][1] : (r == 2) ? zc[k][2] : zc[k][3];
@@ -722,7 +722,7 @@ struct Node {
                 for (int k = 0; k < NINT; ++k) z[k] = fed_p[k * n];
                 fed_p += (size_t)NINT * n;
             } else {
-                const int r = (int)(s & 3);
+                const int r = philox_lane_of(s);
 #pragma unroll
                 for (int k = 0; k < NINT; ++k)
                     z[k] = (r == 0) ? zc[k][0] : (r == 1) ? zc[k][1] : (r == 2) ? zc[k][2] : zc[k][3];
@@ -884,7 +884,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         }
     } else {
         // Blocked loop: steps go in blocks of four aligned to the Philox noise
-        // blocks (s = 4q .. 4q + 3).  A block with no monitor sample before its
+        // blocks (s = 4q + 1 .. 4q + 4).  A block with no monitor sample before its
         // last step runs as straight-line code -- the four steps' normals come
         // from registers, the next block's normals are drawn in between, the
         // monitors only accumulate, and the samples that fall on its last step
@@ -899,7 +899,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         int64_t s = s0 + 1;  // the step to do next
         int ks = 0;
         while (ks < nsteps) {
-            const bool fast = !fed && K >= 4 && (s & 3) == 0 && nsteps - ks >= 4 && node.cd_t >= 4 &&
+            const bool fast = !fed && K >= 4 && philox_lane_of(s) == 0 && nsteps - ks >= 4 && node.cd_t >= 4 &&
                               node.cd_i >= 4 && node.cd_b >= 4 && node.cd_s >= 4;  // uniform over the CTA
             if (fast) {
                 if (since_sync + 4 > K) {
@@ -907,7 +907,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                     __syncthreads();
                 }
                 if (act) {
-                    if (SchemeTraits<SCHEME>::stoch && zq != (s >> 2)) node.philox_block(i, s, node.zc);
+                    if (SchemeTraits<SCHEME>::stoch && zq != philox_block_of(s)) node.philox_block(i, s, node.zc);
                     // variables with a zero sigma draw nothing: their normals stay 0 (0 * z must not see garbage)
                     float zn[M::NINT][4] = {};
 #pragma unroll
@@ -935,7 +935,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
 #pragma unroll
                     for (int r = 0; r < 4; ++r) wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
                 }
-                zq = (s >> 2) + 1;
+                zq = philox_block_of(s) + 1;
                 node.tick(L, 4, act, s + 3, i, n);
                 since_sync += 4;
                 s += 4;
@@ -943,7 +943,8 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
             } else {
                 wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
                 if (act) {
-                    if (SchemeTraits<SCHEME>::stoch && !fed && zq != (s >> 2)) node.philox_block(i, s, node.zc);
+                    if (SchemeTraits<SCHEME>::stoch && !fed && zq != philox_block_of(s))
+                        node.philox_block(i, s, node.zc);
                     float c[NCV], z[M::NINT];
 #pragma unroll
                     for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
@@ -955,7 +956,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                     if (EXT && node.aff_p != nullptr) node.afferent(cnext, n);
                     write(wslot);
                 }
-                zq = s >> 2;
+                zq = philox_block_of(s);
                 node.tick(L, 1, act, s, i, n);
                 if (++since_sync == K) {
                     since_sync = 0;
