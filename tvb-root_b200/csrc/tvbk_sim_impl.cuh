@@ -22,6 +22,7 @@
 // weight) in registers for the whole launch, MAXD >= the largest row degree;
 // with MAXD = 0 it reads them from global memory (L1) every step.
 #pragma once
+#include <type_traits>
 #include <cstdint>
 
 #include "tvbk.h"
@@ -646,8 +647,9 @@ struct Node {
     // Advance the clock by m steps, the last of which is step s, and take the
     // samples that fall on step s (every thread calls it; `act` threads write).
     // m > 1 only when no sample falls on the m - 1 steps before s.
-    __device__ __forceinline__ void tick(const tvbk_launch& L, int m, bool act, int64_t s, int i, int n) {
-        const int nvoi = L.nvoi;
+    // TemporalAverage and SubSample clocks alone (the straight-line block takes
+    // their samples at any of its steps, one step at a time)
+    __device__ __forceinline__ void tick_t(int m, bool act, int n, int nvoi) {
         if (on_t) cd_t -= m;
         if (cd_t == 0) {
             cd_t = t_istep;
@@ -662,6 +664,26 @@ struct Node {
                 tavg_p += (size_t)nvoi * n;
             }
         }
+    }
+
+    __device__ __forceinline__ void tick_s(const tvbk_launch& L, int m, bool act, int n, int nvoi) {
+        if (on_s) cd_s -= m;
+        if (cd_s == 0) {
+            cd_s = s_istep;
+            if (act) {
+#pragma unroll
+                for (int v = 0; v < MV; ++v)
+                    if (v < nvoi) sub_p[v * n] = M::observe(L.voi[v], x);
+                sub_p += (size_t)nvoi * n;
+            }
+        }
+    }
+
+    // ts = false: the TemporalAverage and SubSample clocks were already advanced step by step
+    __device__ __forceinline__ void tick(const tvbk_launch& L, int m, bool act, int64_t s, int i, int n,
+                                         bool ts = true) {
+        const int nvoi = L.nvoi;
+        if (ts) tick_t(m, act, n, nvoi);
         if (on_b) {
             cd_i -= m;
             cd_b -= m;
@@ -683,16 +705,7 @@ struct Node {
             cd_b = b_istep;
             if (act) bold_sample(s, i, n, nvoi);
         }
-        if (on_s) cd_s -= m;
-        if (cd_s == 0) {
-            cd_s = s_istep;
-            if (act) {
-#pragma unroll
-                for (int v = 0; v < MV; ++v)
-                    if (v < nvoi) sub_p[v * n] = M::observe(L.voi[v], x);
-                sub_p += (size_t)nvoi * n;
-            }
-        }
+        if (ts) tick_s(L, m, act, n, nvoi);
     }
 
     // Bold output at step s: (hrf . stock - 1) k1 V0 with the kernel rolled to the current stock position.
@@ -899,44 +912,65 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         int64_t s = s0 + 1;  // the step to do next
         int ks = 0;
         while (ks < nsteps) {
-            const bool fast = !fed && K >= 4 && philox_lane_of(s) == 0 && nsteps - ks >= 4 && node.cd_t >= 4 &&
-                              node.cd_i >= 4 && node.cd_b >= 4 && node.cd_s >= 4;  // uniform over the CTA
+            // TemporalAverage / SubSample samples may fall anywhere in a block, Bold ones only on its last step
+            const bool fast = !fed && K >= 4 && philox_lane_of(s) == 0 && nsteps - ks >= 4 && node.cd_i >= 4 &&
+                              node.cd_b >= 4;  // uniform over the CTA
             if (fast) {
                 if (since_sync + 4 > K) {
                     since_sync = 0;
                     __syncthreads();
                 }
-                if (act) {
-                    if (SchemeTraits<SCHEME>::stoch && zq != philox_block_of(s)) node.philox_block(i, s, node.zc);
-                    // variables with a zero sigma draw nothing: their normals stay 0 (0 * z must not see garbage)
-                    float zn[M::NINT][4] = {};
+                // a TemporalAverage or SubSample sample before the block's last step: the block takes the
+                // samples step by step (a second copy of the block); else its clocks advance at its end
+                const bool inside = node.cd_t < 4 || node.cd_s < 4;  // uniform over the CTA
+                auto block = [&](auto inside_tag) {
+                    constexpr bool IN = decltype(inside_tag)::value;
+                    if (act) {
+                        if (SchemeTraits<SCHEME>::stoch && zq != philox_block_of(s)) node.philox_block(i, s, node.zc);
+                        // variables with a zero sigma draw nothing: their normals stay 0 (0 * z must not see garbage)
+                        float zn[M::NINT][4] = {};
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        float c[NCV], z[M::NINT];
+                        for (int r = 0; r < 4; ++r) {
+                            float c[NCV], z[M::NINT];
 #pragma unroll
-                        for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
-                        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s + r
-                        row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
-                        if (r == 1) node.philox_block(i, s + 4, zn);  // the next block's normals
+                            for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
+                            wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s + r
+                            row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
+                            if (r == 1) node.philox_block(i, s + 4, zn);  // the next block's normals
 #pragma unroll
-                        for (int k = 0; k < M::NINT; ++k) z[k] = node.zc[k][r];
-                        node.integrate(c, z, L.dt, node.stim_at(ks + r));
-                        node.accumulate(L, n);
-                        if (EXT && node.aff_p != nullptr) node.afferent(cnext, n);
-                        write(wslot);
+                            for (int k = 0; k < M::NINT; ++k) z[k] = node.zc[k][r];
+                            node.integrate(c, z, L.dt, node.stim_at(ks + r));
+                            node.accumulate(L, n);
+                            if constexpr (IN) {
+                                node.tick_t(1, true, n, L.nvoi);
+                                node.tick_s(L, 1, true, n, L.nvoi);
+                            }
+                            if (EXT && node.aff_p != nullptr) node.afferent(cnext, n);
+                            write(wslot);
+                        }
+                        if constexpr (SchemeTraits<SCHEME>::stoch) {
+#pragma unroll
+                            for (int k = 0; k < M::NINT; ++k)
+#pragma unroll
+                                for (int r = 0; r < 4; ++r) node.zc[k][r] = zn[k][r];
+                        }
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
+                            if constexpr (IN) {
+                                node.tick_t(1, false, n, L.nvoi);
+                                node.tick_s(L, 1, false, n, L.nvoi);
+                            }
+                        }
                     }
-                    if constexpr (SchemeTraits<SCHEME>::stoch) {
-#pragma unroll
-                        for (int k = 0; k < M::NINT; ++k)
-#pragma unroll
-                            for (int r = 0; r < 4; ++r) node.zc[k][r] = zn[k][r];
-                    }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
-                }
+                    node.tick(L, 4, act, s + 3, i, n, !IN);
+                };
+                if (inside)
+                    block(std::true_type{});
+                else
+                    block(std::false_type{});
                 zq = philox_block_of(s) + 1;
-                node.tick(L, 4, act, s + 3, i, n);
                 since_sync += 4;
                 s += 4;
                 ks += 4;
