@@ -365,8 +365,8 @@ def run_large_network(args, rank, local):
 
 
 # DRAM bytes per instance-step of the simulation kernel on this workload, from the ncu capture
-# of 296 instances x 40 000 steps (dram__bytes_read.sum + dram__bytes_write.sum = 1.797 GB;
-# profiles/sim_kernel_rww_sweep_296i_4s.md); a launch's traffic scales with its instance-steps.
+# of 296 instances x 40 000 steps (dram__bytes_read.sum + dram__bytes_write.sum = 1.797 GB);
+# a launch's traffic scales with its instance-steps.
 NCU_DRAM_BYTES_PER_INSTANCE_STEP = 1.771e9 / (296 * 40000)
 
 

@@ -294,19 +294,21 @@ int tvbk_balloon(const double* x, int32_t T, int64_t nseries, double dt, const d
  * plug-in host that only holds the input and output buffers it was given,
  * or code under a fixed memory budget).  The working memory that
  * tvbk_sim_run takes from the caller -- the ring the kernel advances, the
- * TemporalAverage and Bold accumulators, the Bold 4 ms stock, the descriptor
- * and the status word -- lives in a static device array of
- * TVBK_STATIC_SCRATCH_BYTES; larger instances are rejected with
- * TVBK_ERR_TOO_LARGE.  `inst` is a host struct: inst->ring is the caller's
- * initial ring (device, read only), inst->state the caller's state buffer
- * (read at the start, holds the final state at the end), inst->tavg_acc,
- * bold_acc and bold_stock are ignored, every monitor starts from zero, and
+ * TemporalAverage, Bold, AfferentCoupling and projection-stream
+ * accumulators, the Bold 4 ms stock, the descriptor and the status word --
+ * lives in a static device array of TVBK_STATIC_SCRATCH_BYTES; larger
+ * instances are rejected with TVBK_ERR_TOO_LARGE.  `inst` is a host struct:
+ * inst->ring is the caller's initial ring (device, read only), inst->state
+ * the caller's state buffer (read at the start, holds the final state at the
+ * end), inst->tavg_acc, bold_acc, bold_stock, aff_acc and proj_acc are
+ * ignored, every monitor starts from zero, and
  * all steps from inst->step to inst->step_end run in this call
  * (L->insts, L->status, L->n_inst, L->max_n, L->max_ring_len and
  * L->max_steps are ignored).  status_out, if not NULL, is a device int32
  * that receives the TVBK_STATUS_* bits.  The first call on a device looks up
  * the array's address with that device current; make it before any stream
- * capture.  Calls share the array and keep the last call's contents: calls
+ * capture.  That address does not survive a cudaDeviceReset of the device.
+ * Calls share the array and keep the last call's contents: calls
  * that overlap on the GPU race, so serialise them. */
 int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, int32_t* status_out, void* stream);
 

@@ -748,7 +748,9 @@ def case_projection(R):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference/tvb_library')
+    ap.add_argument('--ref', default=os.environ.get('TVB_REFERENCE_LIBRARY'),
+                    required='TVB_REFERENCE_LIBRARY' not in os.environ,
+                    help='the reference\'s tvb_library source directory (default: $TVB_REFERENCE_LIBRARY)')
     ap.add_argument('--only', nargs='*')
     ap.add_argument('--compact', nargs='*', help='re-save existing fixtures with large inputs hashed')
     args = ap.parse_args()

@@ -9,16 +9,20 @@
 // fixed memory budget, and callers that must not allocate while other work
 // is being recorded.  tvbk_sim_run needs caller-allocated scratch besides the
 // inputs and outputs (the working copy of the delayed-history ring, the
-// TemporalAverage and Bold accumulators, the Bold 4 ms stock, the instance
-// descriptor and its status word).  This variant keeps all of that in
-// g_static_scratch below, TVBK_STATIC_SCRATCH_BYTES bytes per device, and
-// allocates nothing: it calls no cudaMalloc, cudaFree or allocating library
-// routine.
+// TemporalAverage, Bold, AfferentCoupling and projection-stream accumulators,
+// the Bold 4 ms stock, the instance descriptor and its status word).  This
+// variant keeps all of that in g_static_scratch below,
+// TVBK_STATIC_SCRATCH_BYTES bytes per device, and allocates nothing: it calls
+// no cudaMalloc, cudaFree or allocating library routine.  Every accumulator
+// starts each call from zero; the caller's *_acc pointers are not read.
 //
 // The array exists on every GPU that loads the library and stays allocated
 // until the process exits.  Its device address is looked up once per device
 // (cudaGetSymbolAddress, with that device current) by the first call made on
 // that device, so that first call should come before any stream capture.
+// The looked-up address belongs to the device's context of that moment: after
+// a cudaDeviceReset of the device (which this library never calls) it is
+// stale, and the process must not call this entry point on that device again.
 // All calls on a device share the one array and it keeps the contents of the
 // last call: each call re-initialises what must start from zero or from the
 // caller's inputs, and calls whose work overlaps on the GPU (concurrent
@@ -90,9 +94,10 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
         return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: ring_len %d < horizon + sync_every", inst->ring_len);
     if (inst->step_end < inst->step) return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: step_end < step");
 
-    // scratch layout: descriptor | status | tavg_acc | bold_acc | bold_stock | ring | pre_ring
+    // scratch layout: descriptor | status | tavg_acc | bold_acc | bold_stock | aff_acc | proj_acc | ring | pre_ring
     const int64_t n = inst->n, nvoi = L->nvoi;
     const bool tavg = inst->tavg != nullptr, bold = inst->bold != nullptr;
+    const bool aff = inst->aff != nullptr, proj = inst->proj != nullptr;
     if (bold && (!inst->hrf || inst->stock_len <= 0))
         return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: Bold needs hrf and stock_len");
     size_t off = 0;
@@ -107,6 +112,11 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
     off = align256(off + (bold ? nvoi * n * sizeof(double) : 0));
     const size_t o_stock = off;
     off = align256(off + (bold ? (size_t)inst->stock_len * nvoi * n * sizeof(double) : 0));
+    // the AfferentCoupling and projection-stream period sums: both start every call from zero
+    const size_t o_aff = off;
+    off = align256(off + (aff ? (size_t)ncvar * n * sizeof(float) : 0));
+    const size_t o_proj = off;
+    off = align256(off + (proj ? (size_t)nvoi * n * sizeof(float) : 0));
     const size_t zero_bytes = off - o_zero;
     const size_t o_ring = off;
     const int64_t ring_floats = (int64_t)inst->ring_len * n * ncvar;
@@ -143,6 +153,8 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
     d.tavg_acc = tavg ? reinterpret_cast<float*>(base + o_tacc) : nullptr;
     d.bold_acc = bold ? reinterpret_cast<double*>(base + o_bacc) : nullptr;
     d.bold_stock = bold ? reinterpret_cast<double*>(base + o_stock) : nullptr;
+    d.aff_acc = aff ? reinterpret_cast<float*>(base + o_aff) : nullptr;
+    d.proj_acc = proj ? reinterpret_cast<float*>(base + o_proj) : nullptr;
     tvbk_inst* desc = reinterpret_cast<tvbk_inst*>(base + o_desc);
     int32_t* status = reinterpret_cast<int32_t*>(base + o_status);
     cudaStream_t st = (cudaStream_t)stream;
