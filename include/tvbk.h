@@ -184,7 +184,9 @@ typedef struct tvbk_launch {
     int32_t block_threads;       /* CTA size for the edge-parallel gather (multiple of 32, >= max_n, <= 512) */
     int32_t prefetch;            /* 1: issue the gather of step s + 1 before the update of step s (row kernel,
                                   * Linear or SigmoidalJansenRit); needs every delay >= 1 and
-                                  * 1 <= sync_every <= the smallest delay.  2: the same overlap with separate
+                                  * 1 <= sync_every <= the smallest delay.  With rings in shared memory the
+                                  * kernel then stages max_ring_len + TVBK_RING_GUARD slots per instance (the
+                                  * guard slots mirror slots 0..TVBK_RING_GUARD-1).  2: the same overlap with separate
                                   * warps -- ceil(max_n / 32) gather warps sum the rows of step s + 1 while as
                                   * many update warps advance step s (rings in shared memory, row degrees
                                   * <= 64; one CTA barrier per step) */
@@ -239,6 +241,11 @@ int tvbk_sparse_layout(const double* weights, const int32_t* idelays, int32_t n,
  * n regions and ncvar coupling variables.  Host function. */
 int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weight, int32_t nnz,
                     int32_t n, int32_t ncvar, tvbk_edge* edges);
+
+/* Slots past the end of a ring staged in shared memory with prefetch = 1:
+ * they mirror slots 0..TVBK_RING_GUARD-1, so that the gathers of four steps
+ * in a row take one ring address per edge (address + r slots, r <= 3). */
+#define TVBK_RING_GUARD 3
 
 /* Smallest ring length (slots) usable with barrier interval sync_every. */
 int32_t tvbk_ring_len(int32_t horizon, int32_t sync_every);

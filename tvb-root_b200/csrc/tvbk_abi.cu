@@ -275,7 +275,9 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
         // the row kernel stages one pre-applied sigmoid value per (slot, region) for SigmoidalJansenRit
         const int64_t ncv_g = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
-        int64_t b = (int64_t)L->max_ring_len * L->max_n * ncv_g * (int64_t)sizeof(float);
+        // with prefetch 1 the row kernel keeps TVBK_RING_GUARD mirrored slots past the ring's end
+        const int64_t slots = (int64_t)L->max_ring_len + (L->prefetch == 1 && L->lanes <= 1 ? TVBK_RING_GUARD : 0);
+        int64_t b = slots * L->max_n * ncv_g * (int64_t)sizeof(float);
         // separate gather warps pass the sums through a double buffer after the ring
         if (L->prefetch == 2) b = (b + 15) / 16 * 16 + (int64_t)2 * L->max_n * d.ncvar * (int64_t)sizeof(float);
         if (b > kMaxSmemPerBlock || L->max_n > 256)

@@ -220,6 +220,43 @@ struct RegRow {
             post<CF, NCV>(a, cf, c);
         }
     }
+
+    // The couplings of four consecutive gathers, c[r] read at ring times
+    // (time of base_off) + r - d, r = 0..3: one wrapped ring address per edge,
+    // then r slots past it.  Those may run up to three slots past the ring's
+    // end, into the guard slots that mirror slots 0..2 (TVBK_RING_GUARD).
+    // Each gather sums its slots in the same order into the same two partial
+    // sums as sum(), so c[r] equals couple() at base_off + r slots bit for
+    // bit.  Couplings whose pre() ignores x_i only (the prefetching kernel's).
+    __device__ __forceinline__ void couple4(const float* __restrict__ ring, int base_off, int ring_floats,
+                                            int slot_floats, const float* cf, float (*c)[M::NCV]) const {
+        static_assert(CF != CF_GENERIC && CF != CF_DIFFERENCE, "couple4 is for couplings whose pre() ignores x_i");
+        constexpr int NCV = M::NCV;
+        constexpr int NG = GatherTraits<CF, NCV>::NG, GCF = GatherTraits<CF, NCV>::GCF;
+        float a0[4][NG], a1[4][NG];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < NG; ++k) a0[r][k] = a1[r][k] = 0.0f;
+        const char* rb = reinterpret_cast<const char*>(ring);
+        const int base_b = base_off * (int)sizeof(float), ring_b = ring_floats * (int)sizeof(float);
+        const int sb = slot_floats * (int)sizeof(float);
+#pragma unroll
+        for (int k = 0; k < MAXD; ++k) {
+            const int a = gather_addr(base_b, off[k], ring_b);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                accumulate<GCF, NG>((k & 1) ? a1[r] : a0[r], w[k], reinterpret_cast<const float*>(rb + r * sb + a),
+                                    nullptr, cf);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            float s[NG];
+#pragma unroll
+            for (int k = 0; k < NG; ++k) s[k] = a0[r][k] + a1[r][k];
+            post<CF, NCV>(s, cf, c[r]);
+        }
+    }
 };
 
 // Row gather reading the packed edges from global memory every step.
@@ -831,11 +868,20 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     // gather ring: the raw ring (staged in shared memory or in place), or for
     // SigmoidalJansenRit the pre-applied sigmoid values computed from it
     float* ring = SMEM ? smem : (SIGMA ? Ip->pre_ring : Ip->ring);
+    // A ring staged in shared memory for the prefetching loop has TVBK_RING_GUARD
+    // slots past its end that mirror slots 0..GUARD-1 (the four-step gathers of
+    // couple4 read up to three slots past a wrapped address); every write of
+    // one of those slots also goes to its mirror.
+    constexpr bool GUARDED = SMEM && PIPE && MAXD > 0;
+    constexpr int GUARD = GUARDED ? TVBK_RING_GUARD : 0;
     if constexpr (SIGMA) {
         sigma_ring(ring, Ip->ring, RL * n, threadIdx.x, blockDim.x, cf);
+        if constexpr (GUARDED) sigma_ring(ring + ring_floats, Ip->ring, GUARD * n, threadIdx.x, blockDim.x, cf);
         __syncthreads();
     } else if (SMEM) {
         stage_ring(smem, Ip->ring, ring_floats);
+        if constexpr (GUARDED)
+            for (int k = threadIdx.x; k < GUARD * slot_floats; k += blockDim.x) smem[ring_floats + k] = Ip->ring[k];
         __syncthreads();
     }
     RegRow<M, CF, MAXD> row;
@@ -863,9 +909,12 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     auto write = [&](int slot) {
         if constexpr (SIGMA) {
             node.write_ring(Ip->ring + (size_t)slot * n * NCV + i * NCV);
-            ring[slot * slot_floats + i] = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+            const float v = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+            ring[slot * slot_floats + i] = v;
+            if (GUARDED && slot < GUARD) ring[(slot + RL) * slot_floats + i] = v;
         } else {
             node.write_ring(ring + slot * slot_floats + i * NCV);
+            if (GUARDED && slot < GUARD) node.write_ring(ring + (slot + RL) * slot_floats + i * NCV);
         }
     };
     if constexpr (!PIPE) {
@@ -929,13 +978,27 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                         if (SchemeTraits<SCHEME>::stoch && zq != philox_block_of(s)) node.philox_block(i, s, node.zc);
                         // variables with a zero sigma draw nothing: their normals stay 0 (0 * z must not see garbage)
                         float zn[M::NINT][4] = {};
+                        // the couplings of steps s + 1 .. s + 4, all gathered first: they read times
+                        // s + r - d <= s - 1 (d >= d_min >= K >= 4), none written in this block, so the
+                        // four gathers are independent of the block's updates and of each other
+                        float cb[4][NCV];
+                        (void)cb;
+                        if constexpr (GUARDED) {
+                            const int s0slot = (wslot + 1 == RL) ? 0 : wslot + 1;  // slot of time s
+                            row.couple4(ring, s0slot * slot_floats, ring_floats, slot_floats, cf, cb);
+                        }
 #pragma unroll
                         for (int r = 0; r < 4; ++r) {
                             float c[NCV], z[M::NINT];
 #pragma unroll
                             for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
                             wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s + r
-                            row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
+                            if constexpr (GUARDED) {
+#pragma unroll
+                                for (int k = 0; k < NCV; ++k) cnext[k] = cb[r][k];
+                            } else {
+                                row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
+                            }
                             if (r == 1) node.philox_block(i, s + 4, zn);  // the next block's normals
 #pragma unroll
                             for (int k = 0; k < M::NINT; ++k) z[k] = node.zc[k][r];

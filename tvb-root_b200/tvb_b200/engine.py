@@ -267,12 +267,18 @@ class Batch:
         # stage rings in shared memory when the largest fits, shrinking K if that makes it fit
         smem_ok = self.max_n <= 256 and V == 1
         ncg = self.ncvar if gather == 'edge' else self.ncvar_gather
+        self.generic = self.cfun_id in _lib.CFUN_GENERIC
+        # the prefetching row kernel (below) stages RING_GUARD mirrored slots past each ring
+        pipe = (gather not in ('edge', 'split') and V == 1 and dmin >= 1
+                and self.cfun_id != _lib.CFUN_IDS['Difference'] and self.model_id != _lib.MODEL_IDS['Sum']
+                and not self.generic)
+        guard = _lib.RING_GUARD if pipe else 0
         if ring_in_smem is None:
             ring_in_smem = smem_ok
         if ring_in_smem:
-            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, ncg * V, hmax + K) == 0:
+            while K > 1 and self.lib.tvbk_ring_smem_bytes(self.max_n, ncg * V, hmax + K + guard) == 0:
                 K -= 1
-            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, ncg * V, hmax + K) == 0:
+            if not smem_ok or self.lib.tvbk_ring_smem_bytes(self.max_n, ncg * V, hmax + K + guard) == 0:
                 ring_in_smem = False
                 K = dmin + 1 if sync_every is None else max(1, min(int(sync_every), dmin + 1))
         self.sync_every = K
@@ -281,7 +287,6 @@ class Batch:
         self.prefetch = 0
         if gather not in ('auto', 'row', 'edge', 'split'):
             raise ValueError("gather must be 'auto', 'row', 'edge' or 'split'")
-        self.generic = self.cfun_id in _lib.CFUN_GENERIC
         if self.generic and (gather in ('edge', 'split') or V != 1):
             raise ValueError('Sigmoidal, HyperbolicTangent and Kuramoto run on the row gather, one instance '
                              'per CTA')
@@ -306,6 +311,8 @@ class Batch:
                 self.edges_per_thread, self.block_threads, self.sync_every = ep
             elif gather == 'edge':
                 raise ValueError('the edge-parallel gather does not apply to this batch')
+        # mirrored guard slots past a shared-memory ring (prefetch 1 only; the split kernel has none)
+        self.guard = _lib.RING_GUARD if (self.prefetch == 1 and self.ring_in_smem and V == 1) else 0
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
         self.slot_width, self._ring_len = self._choose_slots()
         self._plan()
@@ -356,28 +363,39 @@ class Batch:
         shared memory (one float per ring entry, 32..256 regions): the ring
         of each instance is lengthened to the next multiple of 32 / gcd(n, 32)
         slots (its float count then a multiple of 32), when that keeps the
-        same number of CTAs per SM.  Returns (slot width or 0, ring length of a
-        spec)."""
-        K = self.sync_every
+        same number of CTAs per SM.  With guard slots (the prefetching row
+        kernel) the barrier interval K may be lowered, down to 4, when a
+        shorter padded ring plus its guard keeps more CTAs per SM resident.
+        Returns (slot width or 0, ring length of a spec) and sets sync_every."""
+        K0 = self.sync_every
+        G = self.guard
 
-        def plain(s):
-            return s.conn.horizon + K
+        def plain(K):
+            return lambda s: s.conn.horizon + K
+
+        def padded(K):
+            def f(s):
+                m = 32 // math.gcd(s.conn.n, 32)
+                return -(-(s.conn.horizon + K) // m) * m
+            return f
+
+        def ctas(ring_len):
+            b = (max(ring_len(s) for s in self.specs) + G) * self.max_n * self.ncvar_gather * 4
+            return 0 if b > 227 * 1024 else self.SM_SMEM // (b + self.CTA_RESERVED)
+
         if not (self.ring_in_smem and self.lanes == 1 and not self.edges_per_thread and self.prefetch != 2
                 and self.ncvar_gather == 1 and not self.cluster and 0 < self.max_degree <= 64
                 and all(s.conn.n >= 32 for s in self.specs)):
-            return 0, plain
+            return 0, plain(K0)
         width = 32 if self.max_degree <= 32 else 64
-
-        def padded(s):
-            m = 32 // math.gcd(s.conn.n, 32)
-            return -(-(s.conn.horizon + K) // m) * m
-        old = max(plain(s) for s in self.specs) * self.max_n * 4
-        new = max(padded(s) for s in self.specs) * self.max_n * 4
-        if new > 227 * 1024 or self.SM_SMEM // (new + self.CTA_RESERVED) < self.SM_SMEM // (old + self.CTA_RESERVED):
-            return 0, plain
+        cands = [K0] + (list(range(K0 - 1, 3, -1)) if G and K0 > 4 else [])
+        (occ, K) = max((ctas(padded(K)), K) for K in cands)
+        if occ == 0 or occ < ctas(plain(K0)):
+            return 0, plain(K0)
         if any(s.conn.slot_table(width) is None for s in self.specs):
-            return 0, plain
-        return width, padded
+            return 0, plain(K0)
+        self.sync_every = K
+        return width, padded(K)
 
     CLUSTER_SMEM = 227 * 1024
     CLUSTER_MAX_ROWS = 480
