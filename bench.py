@@ -13,10 +13,16 @@ instances, EulerStochastic dt 0.1 ms, 60 s each (600 000 steps), Bold
 Prints one JSON line.  `value` is region-steps/s of the device path with the
 inputs resident in HBM (kernel launches of the sweep + FC, CUDA events);
 `e2e` is the same metric through the public ParameterSweep API from host
-arrays to host results, transfers included.  Under torchrun each rank runs
-its own 1024-instance shard (weak scaling, no collective on the data path)
-and the time is the max over ranks.  `--impl reference` times the CPU oracle
-(a numpy restatement of the reference's numpy path) on the host cores.
+arrays to host results, transfers included.  Under torchrun with N ranks the
+global sweep is N x 1024 instances (N independent noise realisations of the
+grid: instance g is grid point g % 1024 with Philox stream g) and each rank
+runs its own 1024-instance shard (weak scaling, no collective on the data
+path); the time is the max over ranks.  At N = 1 the line also carries the
+Philox-path parity check against the oracle (Bold, state, FC), the serving
+leg (p50/p99 latency at a stated Poisson rate) and the large-network leg
+(region-steps/s and per-instance error against the float64 oracle).
+`--impl reference` times the CPU oracle (a numpy restatement of the
+reference's numpy path) on the host cores.
 """
 import argparse
 import json
@@ -33,6 +39,7 @@ sys.path.insert(0, os.path.join(HERE, 'tvb-root_b200'))
 import numpy as np  # noqa: E402
 
 METRIC = 'region-steps/sec batched FP32 vs plain, err vs FP64 oracle; p50/p99 sim latency'
+PHILOX_SEED = 42      # the sweep's noise_seed (Additive default)
 UNIT = 'region-steps/s'
 N_REGIONS, DENSITY, L_LO, L_HI, SPEED, SEED = 68, 0.30, 10.0, 200.0, 5.0, 3
 DT = 0.1
@@ -45,18 +52,24 @@ def sweep_grid():
     return gg.reshape(-1), ss.reshape(-1)
 
 
-def make_sweep(instances, length_ms, rank=0, chunk=None, gather='auto', lanes=1):
+def make_sweep(instances, length_ms, rank=0, world=1, chunk=None, gather='auto', lanes=1, select=None):
+    """The sweep of `instances` x `world` global instances: global instance g
+    is grid point g % 1024 with its own Philox stream g (for world > 1, one
+    independent noise realisation of the grid per rank); this process runs
+    shard `rank` of `world` (weak scaling: `instances` per rank), or the
+    global indices in `select`."""
     from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
     from tvb_b200.connectivity import Connectivity
     from tvb_b200.sweep import ParameterSweep
     w, L = synthetic.connectome(N_REGIONS, DENSITY, L_LO, L_HI, seed=SEED)
     G, S = sweep_grid()
-    idx = (np.arange(instances) + rank * instances) % G.size
+    idx = np.arange(instances * world) % G.size
+    where = dict(instances=select) if select is not None else dict(shard=(rank, world))
     sw = ParameterSweep(model=models.ReducedWongWang(), connectivity=Connectivity(w, L, speed=SPEED),
                         coupling=coupling.Linear(), monitors=[monitors.Bold(period=2000.0)],
                         integrator=integrators.EulerStochastic(dt=DT, noise=noise.Additive(nsig=[1e-3])),
                         simulation_length=length_ms, sweep={'coupling.a': G[idx], 'noise.nsig': S[idx]},
-                        chunk_steps=chunk, gather=gather, lanes=lanes)
+                        chunk_steps=chunk, gather=gather, lanes=lanes, **where)
     return sw
 
 
@@ -118,9 +131,10 @@ class ClockSampler:
 # -------------------------------------------------------------- CPU oracle
 
 def _oracle_worker(args):
-    """One reference-equivalent instance on the CPU oracle (numpy), including
-    its per-step normal draws like the reference's RandomState path."""
-    k, n_steps, G, nsig = args
+    """One sweep instance on the CPU oracle (numpy restatement of the
+    reference's numpy path), including its per-step normal draws like the
+    reference's RandomState path; returns the seconds it took."""
+    g, n_steps, G, nsig = args
     os.environ['OMP_NUM_THREADS'] = '1'
     from oracle import tvb_oracle as O
     from tvb_b200 import synthetic
@@ -131,85 +145,109 @@ def _oracle_worker(args):
     hist = O.reference_initial_history(rs, [info['ranges']['S']], H, N_REGIONS)
     t0 = time.perf_counter()
     z = rs.normal(size=(n_steps, 1, N_REGIONS))
-    out, fin = O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic', n_steps,
-                          [O.Monitor('Bold', 2000.0)], hist[:, [0]].astype(np.float32), hist[0], 0, nsig=[nsig],
-                          noise_z=z)
-    el = time.perf_counter() - t0
-    # the all-float64 variant of the same run (float64 history and weights), untimed: the error reference
-    out64, fin64 = O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic',
-                              n_steps, [O.Monitor('Bold', 2000.0)], hist[:, [0]], hist[0], 0, nsig=[nsig],
-                              noise_z=z, history_dtype=np.float64)
-    return el, dict(bold=out[0][1], state=fin['state'], bold64=out64[0][1], state64=fin64['state'])
+    O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic', n_steps,
+               [O.Monitor('Bold', 2000.0)], hist[:, [0]].astype(np.float32), hist[0], 0, nsig=[nsig], noise_z=z)
+    return time.perf_counter() - t0
+
+
+def _warm(_):
+    os.environ['OMP_NUM_THREADS'] = '1'
+    from oracle import tvb_oracle  # noqa: F401
+    from tvb_b200 import synthetic  # noqa: F401
+    return os.getpid()
+
+
+def cpu_sample(pool, cores, n_steps, offset=0):
+    """One sample of the sweep on the host: `cores` instances spread over the
+    (G, nsig) grid (shifted by `offset` grid points), one per core, n_steps
+    each.  Returns (wall seconds of the whole sample, global indices)."""
+    G, S = sweep_grid()
+    pick = (np.linspace(0, G.size - 1, cores).astype(int) + offset) % G.size
+    t0 = time.perf_counter()
+    pool.map(_oracle_worker, [(int(i), n_steps, G[i], S[i]) for i in pick])
+    return time.perf_counter() - t0, pick
+
+
+def _sample_text(cores, n_steps):
+    return ('%d RWW sweep instances spread over the 32 x 32 (G, nsig) grid, one per core, %d steps (%g ms) each, '
+            'oracle numpy path incl. per-step noise draws; value = instances x steps x regions / wall time of the '
+            'sample' % (cores, n_steps, n_steps * DT))
 
 
 def cpu_baseline(n_steps=20000, cores=None):
     import multiprocessing as mp
     cores = cores or os.cpu_count() or 1
-    G, S = sweep_grid()
-    pick = np.linspace(0, G.size - 1, cores).astype(int)
-    ctx = mp.get_context('spawn')
-    t0 = time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_oracle_worker, [(k, n_steps, G[i], S[i]) for k, i in enumerate(pick)])
-    wall = time.perf_counter() - t0
-    times = [r[0] for r in res]
-    rs = cores * n_steps * N_REGIONS
-    cb = {'value': rs / max(times), 'unit': UNIT, 'cores': cores, 'kind': 'port',
-          'sample': '%d RWW sweep instances (one per core), %d steps (%g ms) each, oracle numpy path '
-                    'incl. per-step noise draws; value = instances x steps x regions / slowest instance'
-                    % (cores, n_steps, n_steps * DT), 'wall_s': wall}
-    # kept for the error check against the device (not part of the reported baseline)
-    cb['_check'] = dict(points=pick, n_steps=n_steps, outputs=[r[1] for r in res])
-    return cb
+    with mp.get_context('spawn').Pool(cores) as pool:
+        pool.map(_warm, range(cores))
+        wall, _ = cpu_sample(pool, cores, n_steps)
+    return {'value': cores * n_steps * N_REGIONS / wall, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+            'sample': _sample_text(cores, n_steps), 'wall_s': wall}
 
 
-def error_vs_oracle(check):
-    """The device's float32 run of the CPU-baseline instances, fed the same
-    RandomState normals, against the oracle: the all-float64 variant and the
-    stock (float32 ring) variant.  Relative errors of the final state and of
-    the Bold sample, max over the instances."""
-    import torch
+def _philox_oracle_worker(args):
+    """One sweep instance on the CPU oracle fed the device's Philox normals of
+    its global index: the stock variant (float32 history and weights, like
+    the reference) or the all-float64 one."""
+    g, n_steps, G, nsig, buf0, st0, variant = args
+    os.environ['OMP_NUM_THREADS'] = '1'
     from oracle import tvb_oracle as O
-    from tvb_b200 import _lib, synthetic
-    from tvb_b200.engine import Batch
-    sw = make_sweep(1, check['n_steps'] * DT).configure()
-    sim = sw._sim
+    from tvb_b200 import synthetic
+    w, L = synthetic.connectome(N_REGIONS, DENSITY, L_LO, L_HI, seed=SEED)
+    z = O.philox_normals(PHILOX_SEED, g, np.arange(1, n_steps + 1), 1, N_REGIONS)
+    # the initial history as the reference draws it (float64; the stock variant keeps it in float32)
+    idl, H = O.integer_delays(L, SPEED, DT)
+    h64 = O.reference_initial_history(np.random.RandomState(PHILOX_SEED),
+                                      [O.MODEL_INFO['ReducedWongWang']['ranges']['S']], H, N_REGIONS)
+    assert np.array_equal(h64[:, [0]].astype(np.float32), buf0) and np.array_equal(h64[0], st0)
+    kw = dict(history_dtype=np.float64) if variant == 'fp64' else {}
+    hist = h64[:, [0]] if variant == 'fp64' else buf0
+    out, fin = O.simulate('ReducedWongWang', {}, w, L, SPEED, DT, 'Linear', {'a': G}, 'EulerStochastic', n_steps,
+                          [O.Monitor('Bold', 2000.0)], hist, st0, 0, nsig=[nsig], noise_z=z, **kw)
+    bold = np.asarray(out[0][1])
+    return g, variant, bold.reshape(bold.shape[0], -1), np.asarray(fin['state']).reshape(-1)
+
+
+def philox_check(n_inst, n_steps, cores):
+    """The timed path's parity: the sweep's own kernel, Philox noise and
+    straight-line blocks, on `n_inst` instances spread over the grid for
+    `n_steps` steps (at least 3 Bold samples, so FC is defined), against the
+    CPU oracle fed the same Philox normals -- the stock and the all-float64
+    variants.  Max relative error of Bold and final state per result, and
+    max |dFC| (device FC kernel vs numpy.corrcoef of the oracle's Bold)."""
+    import multiprocessing as mp
     G, S = sweep_grid()
-    n_steps = check['n_steps']
-    rs = np.random.RandomState(42)
-    H = sim._conn.horizon
-    info = O.MODEL_INFO['ReducedWongWang']
-    hist = O.reference_initial_history(rs, [info['ranges']['S']], H, N_REGIONS)
-    z = rs.normal(size=(n_steps, 1, N_REGIONS)).astype(np.float32)
-    specs = []
-    for k, i in enumerate(check['points']):
-        spec, _ = sim.instance_spec(n_steps)
-        spec.ring0 = hist[:, [0]].astype(np.float32)
-        spec.state0 = hist[0]
-        spec.cfun = [float(G[i]), 0.0]
-        from tvb_b200.simulator import noise_sigma
-        spec.sigma = noise_sigma(np.array([S[i]]), 1, N_REGIONS, DT)
-        spec.noise_fed = z
-        specs.append(spec)
-    b = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, _lib.NOISE_FED, DT, sim._voi_codes, specs)
-    b.run()
-    outs = b.outputs_host()
+    pick = np.linspace(0, G.size - 1, n_inst).round().astype(np.int64)
+    sw = make_sweep(G.size, n_steps * DT, select=pick).configure()
+    buf0 = sw._sim.history_buffer[..., 0].copy()
+    st0 = sw._sim.current_state[..., 0].copy()
+    res = sw.run(fc=True)
+    kern = sw.batch.launch_struct(1)
+    dev_state = np.stack([sw.batch.state(k)[0] for k in range(len(pick))])
+    tasks = [(int(g), n_steps, float(G[g]), float(S[g]), buf0, st0, v) for g in pick for v in ('stock', 'fp64')]
+    t0 = time.perf_counter()
+    with mp.get_context('spawn').Pool(min(cores, len(tasks))) as pool:
+        outs = pool.map(_philox_oracle_worker, tasks)
+    wall = time.perf_counter() - t0
+    ref = {(g, v): (bold, st) for g, v, bold, st in outs}
     err = {}
-    for tag, bkey, skey in (('fp64', 'bold64', 'state64'), ('stock', 'bold', 'state')):
-        bm, sm, srms = 0.0, 0.0, 0.0
-        for k, ref in enumerate(check['outputs']):
-            rb = np.asarray(ref[bkey])
-            if rb.size:   # a sample needs at least one Bold period (20 000 steps)
-                bo = outs[k]['bold'][:, 0]
-                bm = max(bm, float(np.abs(bo - rb.reshape(bo.shape)).max() / np.abs(rb).max()))
-            st = b.state(k)[0]
-            rsx = np.asarray(ref[skey])[0]
-            d = st - rsx
-            sm = max(sm, float(np.abs(d).max() / np.abs(rsx).max()))
-            srms = max(srms, float(np.sqrt(np.mean(d ** 2)) / np.sqrt(np.mean(rsx ** 2))))
-        err[tag] = {'bold_max_rel': bm, 'state_max_rel': sm, 'state_rms_rel': srms}
-    return {'instances': len(specs), 'steps': n_steps, 'noise': 'the oracle\'s RandomState normals fed to the '
-            'device', 'vs_all_fp64_oracle': err['fp64'], 'vs_stock_oracle': err['stock']}
+    for v in ('stock', 'fp64'):
+        bm = sm = fm = 0.0
+        per = []
+        for k, g in enumerate(pick):
+            rb, rs = ref[(int(g), v)]
+            db = res['bold'][k][:, 0, :]
+            e_b = float(np.abs(db - rb).max() / np.abs(rb).max())
+            e_s = float(np.abs(dev_state[k] - rs).max() / np.abs(rs).max())
+            e_f = float(np.abs(res['fc'][k] - np.corrcoef(rb.T)).max()) if rb.shape[0] >= 3 else None
+            bm, sm = max(bm, e_b), max(sm, e_s)
+            fm = max(fm, e_f) if e_f is not None else fm
+            per.append({'instance': int(g), 'bold_max_rel': e_b, 'state_max_rel': e_s, 'fc_max_abs': e_f})
+        err[v] = {'bold_max_rel': bm, 'state_max_rel': sm, 'fc_max_abs': fm, 'per_instance': per}
+    return {'instances': [int(g) for g in pick], 'steps': n_steps, 'bold_samples': int(res['bold'][0].shape[0]),
+            'noise': 'philox (the timed path: straight-line blocks, prefetch %d); the oracle fed the same '
+                     'Philox normals' % kern.prefetch,
+            'vs_all_fp64_oracle': err['fp64'], 'vs_stock_oracle': err['stock'], 'oracle_wall_s': wall,
+            'nonfinite_instances': int((res['status'] != 0).sum())}
 
 
 # ------------------------------------------------------------ plain form
@@ -280,87 +318,170 @@ def serving_sim(model, n, dt, length, seed):
                      simulation_length=length).configure()
 
 
-def run_serving(args, rank, local):
-    """Serve a Poisson stream of simulation requests (continuous batching) and
-    print sims/s with p50/p99 latency (arrival to result on the host)."""
+def serving_leg(requests, rate, chunk, local, clocks=True):
+    """Serve a Poisson stream of `requests` simulation requests at `rate` per
+    second (continuous batching); sims/s with p50/p99 latency (arrival to
+    result on the host), region-steps/s and device memory."""
     import torch
     from tvb_b200.serving import SimulationServer
     torch.cuda.set_device(local)
-    plan = serving_plan(args.requests, args.rate)
+    plan = serving_plan(requests, rate)
     sims = [serving_sim(m, n, dt, length, seed=1000 + k) for k, (_, m, n, dt, length) in enumerate(plan)]
-    srv = SimulationServer(chunk_steps=args.chunk or 4000, device=torch.device('cuda', local))
+    srv = SimulationServer(chunk_steps=chunk or 4000, device=torch.device('cuda', local))
     arrivals = [(t, (lambda server, s=s: server.submit(s))) for (t, *_), s in zip(plan, sims)]
-    sampler = ClockSampler(local)
-    sampler.start()
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.start()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     srv.run(arrivals=arrivals, timeout=1800.0)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
-    clocks = sampler.stop()
+    clk = sampler.stop() if sampler else None
     st = srv.stats()
     bad = [dict(zip(('model', 'regions', 'dt_ms', 'length_ms'), plan[k][1:]), seed=1000 + k, status=r.status)
            for k, r in sorted(srv.requests.items()) if r.status]
-    line = {'metric': 'serving sims/s with p50/p99 latency (continuous batching)', 'value': st['sims_per_s'],
-            'unit': 'sims/s', 'n_gpus': 1, 'steps': args.requests, 'warmup': 0, 'ms_per_step': 1e3 * wall / args.requests,
-            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+    leg = {'requests': requests, 'rate_per_s': rate, 'sims_per_s': st['sims_per_s'],
+           'latency_p50_s': st['latency_p50_s'], 'latency_p99_s': st['latency_p99_s'],
+           'latency_mean_s': st['latency_mean_s'], 'region_steps_per_s': st['region_steps_per_s'],
+           'memory_budget_bytes': st['memory_budget_bytes'], 'memory_peak_bytes': st['memory_peak_bytes'],
+           'memory_mean_bytes': st['memory_mean_bytes'], 'groups': st['groups'], 'gpu_launches': st['launches'],
+           'nonfinite_requests': len(bad), 'nonfinite': bad[:16], 'wall_s': wall,
+           'workload': 'Poisson arrivals; each request: connectome of %s regions, model G2D / JR / RWW, duration '
+                       'U(1, 60) s, dt 0.05 or 0.1 ms, float32 state' % sorted(SERVE_SIZES),
+           'chunk_steps': srv.chunk_steps}
+    if clk:
+        leg['clocks'] = clk
+    return leg
+
+
+def run_serving(args, rank, local):
+    leg = serving_leg(args.requests, args.rate, args.chunk, local)
+    line = {'metric': 'serving sims/s with p50/p99 latency (continuous batching)', 'value': leg['sims_per_s'],
+            'unit': 'sims/s', 'n_gpus': 1, 'steps': args.requests, 'warmup': 0,
+            'ms_per_step': 1e3 * leg['wall_s'] / args.requests, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
             'config': {'workload': 'serving_poisson', 'requests': args.requests, 'rate_per_s': args.rate,
                        'sizes': sorted(SERVE_SIZES), 'models': ['G2D', 'JR', 'RWW'], 'duration_ms': [1000, 60000],
-                       'dt_ms': [0.05, 0.1], 'chunk_steps': srv.chunk_steps, 'state': 'f32'},
-            'latency_p50_s': st['latency_p50_s'], 'latency_p99_s': st['latency_p99_s'],
-            'latency_mean_s': st['latency_mean_s'], 'region_steps_per_s': st['region_steps_per_s'],
-            'memory_budget_bytes': st['memory_budget_bytes'], 'memory_peak_bytes': st['memory_peak_bytes'],
-            'memory_mean_bytes': st['memory_mean_bytes'], 'groups': st['groups'], 'gpu_launches': st['launches'],
-            'nonfinite_requests': len(bad), 'nonfinite': bad[:16], 'wall_s': wall}
-    if clocks:
-        line['clocks'] = clocks
+                       'dt_ms': [0.05, 0.1], 'chunk_steps': leg['chunk_steps'], 'state': 'f32'}}
+    line.update({k: v for k, v in leg.items() if k not in ('workload', 'chunk_steps', 'requests', 'rate_per_s')})
     print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------- large network
 
-def run_large_network(args, rank, local):
+EPI_N, EPI_DT = 998, 0.05
+
+
+def large_network_sweep(length_scale=1.0, check_ms=None, gather='auto', cluster='auto'):
     """Epileptor, 998 regions (10 % density, tract lengths 5-300 mm, speed
     3 mm/ms), Difference coupling, HeunDeterministic dt 0.05 ms, 16 instances
     with x0 uniform in [-2.4, -1.6] per region and uneven lengths of 2-20 s
-    in one launch, TemporalAverage 1 ms; region-steps/s of the device run."""
-    import torch
+    (times length_scale) in one launch, TemporalAverage 1 ms.  check_ms: all
+    16 instances for the first check_ms ms instead (the error check)."""
     from tvb_b200 import coupling, integrators, models, monitors, synthetic
     from tvb_b200.connectivity import Connectivity
     from tvb_b200.sweep import ParameterSweep
-    torch.cuda.set_device(local)
-    w, L = synthetic.connectome(998, 0.10, 5.0, 300.0, seed=4)
-    rng = np.random.default_rng(14 + rank)
-    x0 = rng.uniform(-2.4, -1.6, (16, 998))
-    lengths = np.linspace(2000.0, 20000.0, 16) * (args.length / 60000.0)
-    np.random.seed(15 + rank)
+    w, L = synthetic.connectome(EPI_N, 0.10, 5.0, 300.0, seed=4)
+    x0 = np.random.default_rng(14).uniform(-2.4, -1.6, (16, EPI_N))
+    lengths = np.linspace(2000.0, 20000.0, 16) * length_scale
+    np.random.seed(15)
+    sweep = {'model.x0': x0} if check_ms else {'model.x0': x0, 'simulation_length': lengths}
     sw = ParameterSweep(model=models.Epileptor(), connectivity=Connectivity(w, L, speed=3.0),
-                        coupling=coupling.Difference(), integrator=integrators.HeunDeterministic(dt=0.05),
-                        monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=float(lengths.max()),
-                        sweep={'model.x0': x0, 'simulation_length': lengths}, gather=args.gather,
-                        cluster=args.cluster if args.cluster == 'auto' else int(args.cluster)).configure()
+                        coupling=coupling.Difference(), integrator=integrators.HeunDeterministic(dt=EPI_DT),
+                        monitors=[monitors.TemporalAverage(period=1.0)],
+                        simulation_length=float(check_ms or lengths.max()), sweep=sweep, gather=gather,
+                        cluster=cluster if cluster == 'auto' else int(cluster)).configure()
+    return sw, x0, lengths
+
+
+def _epileptor_oracle_worker(args):
+    """One large-network instance on the CPU oracle (TemporalAverage 1 ms),
+    stock (float32 history) or all-float64, from the configured history."""
+    k, x0, n_steps, buf0, st0, variant = args
+    os.environ['OMP_NUM_THREADS'] = '1'
+    from oracle import tvb_oracle as O
+    from tvb_b200 import synthetic
+    w, L = synthetic.connectome(EPI_N, 0.10, 5.0, 300.0, seed=4)
+    kw = dict(history_dtype=np.float64) if variant == 'fp64' else {}
+    out, _ = O.simulate('Epileptor', {'x0': x0}, w, L, 3.0, EPI_DT, 'Difference', {'a': 0.1}, 'HeunDeterministic',
+                        n_steps, [O.Monitor('TemporalAverage', 1.0)], buf0, st0, 0, **kw)
+    return k, variant, np.asarray(out[0][1])
+
+
+def large_network_error(check_ms, cores):
+    """Per-instance error of the device's float32 run against the oracle
+    (stock and all-float64) over the first check_ms ms: max relative error of
+    the TemporalAverage within the first 20, 40, ... ms (the coupled
+    Epileptor is chaotic, so the error grows with time)."""
+    import multiprocessing as mp
+    sw, x0, _ = large_network_sweep(check_ms=check_ms)
+    buf0 = sw._sim.history_buffer[..., 0].copy()
+    st0 = sw._sim.current_state[..., 0].copy()
+    res = sw.run(fc=False)
+    n_steps = sw.n_steps
+    tasks = [(k, x0[k], n_steps, buf0, st0, v) for k in range(len(x0)) for v in ('stock', 'fp64')]
+    t0 = time.perf_counter()
+    with mp.get_context('spawn').Pool(min(cores, len(tasks))) as pool:
+        outs = pool.map(_epileptor_oracle_worker, tasks)
+    wall = time.perf_counter() - t0
+    ref = {(k, v): y for k, v, y in outs}
+    windows = [m for m in range(20, int(check_ms) + 1, 20)]
+    per = []
+    for k in range(len(x0)):
+        dev = res['tavg'][k].astype(np.float64)
+        e = {'instance': k}
+        for v in ('fp64', 'stock'):
+            r = ref[(k, v)].reshape(dev.shape)
+            scale = np.abs(r).max()
+            e['vs_%s' % ('all_fp64' if v == 'fp64' else 'stock')] = {
+                '%dms' % m: float(np.abs(dev[:m] - r[:m]).max() / scale) for m in windows}
+        per.append(e)
+    worst = {v: {'%dms' % m: max(p[v]['%dms' % m] for p in per) for m in windows}
+             for v in ('vs_all_fp64', 'vs_stock')}
+    return {'check_ms': check_ms, 'metric': 'max |device - oracle| / max |oracle| of TemporalAverage(1 ms) over '
+            'the first t ms, from the same configured history', 'max_over_instances': worst, 'per_instance': per,
+            'nonfinite_instances': int((res['status'] != 0).sum()), 'oracle_wall_s': wall}
+
+
+def large_network_leg(steps, warmup, local, length_scale=1.0, gather='auto', cluster='auto'):
+    """Region-steps/s of the 16-instance large-network batch on the device."""
+    import torch
+    torch.cuda.set_device(local)
+    sw, x0, lengths = large_network_sweep(length_scale, gather=gather, cluster=cluster)
     b = sw.build()
     b.snapshot()
     st = torch.cuda.current_stream()
     ms = []
-    for k in range(args.warmup + args.steps):
+    for k in range(warmup + steps):
         b.reset()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         sw.run_device()
         e1.record(st)
         torch.cuda.synchronize()
-        if k >= args.warmup:
+        if k >= warmup:
             ms.append(e0.elapsed_time(e1))
-    steps = sw.n_steps_each.sum()
+    steps_total = int(sw.n_steps_each.sum())
     t = float(np.mean(ms)) / 1e3
-    line = {'metric': 'region-steps/sec, large-network batch', 'value': float(steps * 998 / t), 'unit': UNIT,
-            'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t,
+    return {'value': float(steps_total * EPI_N / t), 'unit': UNIT, 'ms_per_step': 1e3 * t, 'steps': steps,
+            'warmup': warmup, 'instances': 16, 'regions': EPI_N, 'nnz': int(sw._sim._conn.nnz), 'dt_ms': EPI_DT,
+            'lengths_ms': lengths.tolist(), 'cluster_ctas_per_instance': b.cluster, 'sync_every': b.sync_every,
+            'nonfinite_instances': int((b.status() != 0).sum()), 'gpu_launches': steps * b.last_launches}
+
+
+def run_large_network(args, rank, local):
+    leg = large_network_leg(args.steps, args.warmup, local, args.length / 60000.0, args.gather, args.cluster)
+    line = {'metric': 'region-steps/sec, large-network batch', 'value': leg['value'], 'unit': UNIT,
+            'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': leg['ms_per_step'],
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': 'epileptor_998r_16i_uneven_2-20s', 'instances': 16, 'regions': 998,
-                       'nnz': int(sw._sim._conn.nnz), 'dt_ms': 0.05, 'lengths_ms': lengths.tolist(),
-                       'cluster_ctas_per_instance': b.cluster, 'sync_every': b.sync_every},
-            'nonfinite_instances': int((b.status() != 0).sum()), 'gpu_launches': args.steps}
+            'config': {'workload': 'epileptor_998r_16i_uneven_2-20s', 'instances': 16, 'regions': EPI_N,
+                       'nnz': leg['nnz'], 'dt_ms': EPI_DT, 'lengths_ms': leg['lengths_ms'],
+                       'cluster_ctas_per_instance': leg['cluster_ctas_per_instance'],
+                       'sync_every': leg['sync_every']},
+            'nonfinite_instances': leg['nonfinite_instances'], 'gpu_launches': leg['gpu_launches']}
+    if args.check_ms > 0:
+        line['error_vs_fp64_oracle'] = large_network_error(args.check_ms, os.cpu_count() or 1)
     print(json.dumps(line), flush=True)
 
 
@@ -373,16 +494,33 @@ NCU_DRAM_BYTES_PER_INSTANCE_STEP = 1.771e9 / (296 * 40000)
 # --------------------------------------------------------------------- main
 
 def run_reference(args, rank):
+    """The reference arm: the oracle port of the reference's numpy path on all
+    host cores.  Each of the W + K steps is one sample (cpu_sample, a
+    different stratified subset of the grid each step); ms_per_step is the
+    measured wall time of a timed sample."""
     if rank != 0:
         return
-    cb = cpu_baseline(n_steps=args.cpu_steps)
-    cb.pop('_check')
-    ms = 1e3 * cb['cores'] * args.cpu_steps * N_REGIONS / cb['value']
-    line = {'metric': METRIC, 'value': cb['value'], 'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    walls = []
+    with mp.get_context('spawn').Pool(cores) as pool:
+        pool.map(_warm, range(cores))
+        for k in range(args.warmup + args.steps):
+            wall, _ = cpu_sample(pool, cores, args.cpu_steps, offset=7 * k)
+            if k >= args.warmup:
+                walls.append(wall)
+    t = float(np.mean(walls))
+    value = cores * args.cpu_steps * N_REGIONS / t
+    full = 1024 * 600000 * N_REGIONS / value
+    cb = {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port', 'sample': _sample_text(cores, args.cpu_steps)}
+    line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * t, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
-            'config': {'workload': 'rww_sweep_68r_1024i_60s_bold_fc', 'sample_only': True},
-            'cpu_baseline': cb, 'e2e': {'value': cb['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0,
+            'config': {'workload': 'rww_sweep_68r_1024i_60s_bold_fc', 'step': 'one sample: ' + cb['sample'],
+                       'extrapolation': 'the numpy path costs the same per step whatever the state, so the '
+                                        'sample rate is the rate of the full 1024 x 600 000-step sweep, which '
+                                        'would take %.0f s on these cores' % full},
+            'cpu_baseline': cb, 'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
                                         'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
@@ -410,6 +548,12 @@ def main():
     ap.add_argument('--cluster', default='auto', help='CTAs per instance (large-network workload)')
     ap.add_argument('--requests', type=int, default=48, help='serving: number of requests')
     ap.add_argument('--rate', type=float, default=4.0, help='serving: Poisson arrival rate (requests/s)')
+    ap.add_argument('--check-steps', type=int, default=80000,
+                    help='steps of the Philox-path parity check against the oracle (0 skips it)')
+    ap.add_argument('--check-ms', type=float, default=60.0,
+                    help='large network: ms of the per-instance error check against the oracle (0 skips it)')
+    ap.add_argument('--no-legs', action='store_true',
+                    help='sweep only: no serving and large-network legs in the line')
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -443,8 +587,9 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    sw = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk, gather=args.gather,
-                    lanes=args.lanes if args.lanes == 'auto' else int(args.lanes)).configure()
+    lanes = args.lanes if args.lanes == 'auto' else int(args.lanes)
+    sw = make_sweep(args.instances, args.length, rank=rank, world=world, chunk=args.chunk, gather=args.gather,
+                    lanes=lanes).configure()
     batch = sw.build()
     batch.snapshot()
     n_steps = sw.n_steps
@@ -488,8 +633,8 @@ def main():
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
         s0.record(st)
-        sw2 = make_sweep(args.instances, args.length, rank=rank, chunk=args.chunk, gather=args.gather,
-                    lanes=args.lanes if args.lanes == 'auto' else int(args.lanes)).configure()
+        sw2 = make_sweep(args.instances, args.length, rank=rank, world=world, chunk=args.chunk,
+                         gather=args.gather, lanes=lanes).configure()
         res = sw2.run(fc=True)
         s1.record(st)
         torch.cuda.synchronize()
@@ -500,10 +645,16 @@ def main():
     if not e2e_times:
         e2e_times = [float('inf')]
     plain = plain_form(args.plain_steps, rank, args.gather) if args.plain_steps > 0 else None
-    errs = None
-    if cb is not None:
-        check = cb.pop('_check')
-        errs = error_vs_oracle(check)
+    errs = serving = large = None
+    if rank == 0 and world == 1:
+        cores = os.cpu_count() or 1
+        if args.check_steps > 0:
+            errs = philox_check(16, args.check_steps, cores)
+        if not args.no_legs:
+            serving = serving_leg(args.requests, args.rate, None, local, clocks=False)
+            large = large_network_leg(1, 1, local)
+            if args.check_ms > 0:
+                large['error_vs_fp64_oracle'] = large_network_error(args.check_ms, cores)
 
     if world > 1:
         tt = torch.tensor([t_dev, t_kern, float(np.median(e2e_times))], device='cuda', dtype=torch.float64)
@@ -525,12 +676,16 @@ def main():
     peak_src = ('measured HBM copy bandwidth (of measured)' if 'hbm_gbs' in peaks
                 else 'the pool\'s earlier HBM measurement, 6650 GB/s (of fallback: no measured peaks file)')
     achieved = gather_bytes / t_kern / 1e9
+    # the rings live in shared memory: the same bytes against its nominal bandwidth (128 B per clock per SM)
+    sm_mhz = (clocks or {}).get('sm_mhz') or float(peaks.get('sm_max_mhz', 1965.0))
+    smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e9
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 * t_dev / args.steps, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
             'config': {'workload': 'rww_sweep_68r_1024i_60s_bold_fc', 'instances_per_gpu': args.instances,
+                       'instances_total': args.instances * world,
                        'regions': N_REGIONS, 'nnz': nnz, 'dt_ms': DT, 'sim_ms': args.length, 'steps': n_steps,
                        'bold_tr_ms': 2000.0, 'fc': True, 'noise': 'philox',
                        'parallelism': 'instances sharded over ranks' if world > 1 else 'single gpu',
@@ -549,7 +704,11 @@ def main():
                                  'kernel time; peak = %s; traffic = ncu '
                                  'DRAM bytes per launch, scaled from a 296-instance x 40 000-step capture; the '
                                  'rings are staged in shared memory, so DRAM carries only staging and Bold'
-                                 % peak_src},
+                                 % peak_src,
+                         'smem': {'achieved': achieved, 'peak': smem_peak, 'unit': 'GB/s', 'frac': achieved / smem_peak,
+                                  'note': 'the same algorithmic bytes against the shared-memory bandwidth the '
+                                          'gather reads: 148 SMs x 128 B per clock at the sampled SM clock '
+                                          '(nominal, not measured)'}},
             'gpu_launches': launches_per_step * args.steps,
             'kernel_ms_per_step': 1e3 * t_kern,
             'nonfinite_instances': int((status != 0).sum()),
@@ -562,6 +721,10 @@ def main():
             line['plain_single_instance'] = plain
         if errs:
             line['error_vs_fp64_oracle'] = errs
+        if serving:
+            line['serving'] = serving
+        if large:
+            line['large_network'] = large
         if cb:
             line['cpu_baseline'] = cb
         print(json.dumps(line), flush=True)

@@ -186,7 +186,11 @@ typedef struct tvbk_launch {
                                   * Linear or SigmoidalJansenRit); needs every delay >= 1 and
                                   * 1 <= sync_every <= the smallest delay.  With rings in shared memory the
                                   * kernel then stages max_ring_len + TVBK_RING_GUARD slots per instance (the
-                                  * guard slots mirror slots 0..TVBK_RING_GUARD-1).  2: the same overlap with separate
+                                  * guard slots mirror slots 0..TVBK_RING_GUARD-1).  3: as 1, and with rings in
+                                  * shared memory the straight-line blocks of four steps gather the next
+                                  * block's couplings while they advance their own; needs
+                                  * 4 <= sync_every <= the smallest delay - 3 (elsewhere it acts as 1).
+                                  * 2: the same overlap as 1 with separate
                                   * warps -- ceil(max_n / 32) gather warps sum the rows of step s + 1 while as
                                   * many update warps advance step s (rings in shared memory, row degrees
                                   * <= 64; one CTA barrier per step) */
@@ -242,7 +246,7 @@ int tvbk_sparse_layout(const double* weights, const int32_t* idelays, int32_t n,
 int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weight, int32_t nnz,
                     int32_t n, int32_t ncvar, tvbk_edge* edges);
 
-/* Slots past the end of a ring staged in shared memory with prefetch = 1:
+/* Slots past the end of a ring staged in shared memory with prefetch = 1 or 3:
  * they mirror slots 0..TVBK_RING_GUARD-1, so that the gathers of four steps
  * in a row take one ring address per edge (address + r slots, r <= 3). */
 #define TVBK_RING_GUARD 3

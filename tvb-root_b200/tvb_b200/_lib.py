@@ -32,7 +32,7 @@ NOISE_NONE, NOISE_FED, NOISE_PHILOX = 0, 1, 2
 MAX_REGIONS = 1024
 MAX_VOI = 8
 STATIC_SCRATCH_BYTES = 8 * 1024 * 1024
-# mirrored slots past the end of a ring staged in shared memory with prefetch = 1 (TVBK_RING_GUARD)
+# mirrored slots past the end of a ring staged in shared memory with prefetch = 1 or 3 (TVBK_RING_GUARD)
 RING_GUARD = 3
 
 

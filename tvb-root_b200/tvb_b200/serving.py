@@ -208,7 +208,8 @@ class SimulationServer:
         L.sync_every = min(p.sync_every for p in plans)
         L.ring_in_smem = 1 if all(p.ring_in_smem for p in plans) else 0
         L.max_degree = max(p.max_degree for p in plans)
-        L.prefetch = 1 if all(p.prefetch for p in plans) else 0
+        pf = {p.prefetch for p in plans}   # one value per group (the group key holds it)
+        L.prefetch = pf.pop() if len(pf) == 1 else (1 if all(p.prefetch for p in plans) else 0)
         L.lanes = 1
         L.cluster = p0.cluster
         L.cluster_edges = max(p.cluster_edges for p in plans)

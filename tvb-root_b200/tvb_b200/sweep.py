@@ -35,11 +35,21 @@ class ParameterSweep:
     'reference' feeds every instance the reference's RandomState stream (the
     same for all, as separate reference runs with the default seed would
     draw), which is for parity checks on short runs.
+
+    Sharding: the swept values define the global instance list, instance g
+    being what the framework's parameter-space exploration runs as operation
+    g.  `shard=(rank, world)` runs the rank-th of `world` contiguous, balanced
+    parts of that list (one process per GPU, no collective while it runs);
+    `instances=` runs an explicit list of global indices instead.  An
+    instance's Philox stream is keyed by its global index, so it draws the
+    same noise whichever process runs it, and results come back in the order
+    of `self.instances` ('instances' in run()'s result); gather_sweep()
+    reassembles the shards on one rank in global order.
     """
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
                  noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
-                 gather='auto', lanes=1, cluster='auto', stimulus=None):
+                 gather='auto', lanes=1, cluster='auto', stimulus=None, shard=None, instances=None):
         self.model = adopt_model(model)
         self.stimulus = stimulus
         self.connectivity = adopt_connectivity(connectivity)
@@ -51,7 +61,11 @@ class ParameterSweep:
         sizes = {len(v) for v in self.sweep.values()}
         if len(sizes) != 1:
             raise ValueError('all swept parameters need the same number of values')
-        self.n_instances = sizes.pop()
+        self.n_global = sizes.pop()
+        self.instances = shard_instances(self.n_global, shard, instances)
+        self.n_instances = len(self.instances)
+        if self.n_instances == 0:
+            raise ValueError('this shard holds no instances')
         self.noise_source = noise_source
         self.chunk_steps = chunk_steps
         self.device = device
@@ -86,7 +100,7 @@ class ParameterSweep:
         specs = []
         lengths = self.sweep.get('simulation_length')
         if lengths is not None:
-            self.n_steps_each = np.ceil(lengths / self.integrator.dt).astype(np.int64)
+            self.n_steps_each = np.ceil(lengths[self.instances] / self.integrator.dt).astype(np.int64)
             self.n_steps = int(self.n_steps_each.max())
         else:
             self.n_steps_each = np.full(self.n_instances, self.n_steps, dtype=np.int64)
@@ -97,7 +111,7 @@ class ParameterSweep:
             sim._prepare_stimulus()
             stim = sim.stimulus_spec(self.n_steps)
             sim.simulation_length = self.simulation_length
-        for i in range(self.n_instances):
+        for i, g in enumerate(self.instances):
             params = base_params
             cf = self.coupling.kernel_params()
             sigma = sim._sigma
@@ -107,22 +121,22 @@ class ParameterSweep:
                 if part == 'model':
                     if params is base_params:
                         params = base_params.copy()
-                    params[pidx[name]] = np.asarray(vals[i], dtype=np.float32)
+                    params[pidx[name]] = np.asarray(vals[g], dtype=np.float32)
                 elif part == 'coupling':
                     cf = list(cf)
-                    cf[cnames.index(name)] = float(vals[i])
+                    cf[cnames.index(name)] = float(vals[g])
                 elif part == 'noise' and name == 'nsig':
-                    sigma = noise_sigma(np.array([vals[i]]), sim.nint, n, self.integrator.dt)
+                    sigma = noise_sigma(np.array([vals[g]]), sim.nint, n, self.integrator.dt)
                 elif key == 'simulation_length':
                     pass
                 elif key == 'stimulus.weight':
-                    stim_i = dict(stim, weight=np.asarray(vals[i], dtype=np.float64).reshape(-1))
+                    stim_i = dict(stim, weight=np.asarray(vals[g], dtype=np.float64).reshape(-1))
                 else:
                     raise ValueError('cannot sweep %s' % key)
             spec = InstanceSpec(conn, sim.history_buffer[..., 0], sim.current_state[..., 0], params, cf,
                                 int(self.n_steps_each[i]), step0=sim.current_step, sigma=sigma, noise_fed=None,
                                 seed=self.integrator.noise.noise_seed if self.integrator.stochastic else 0,
-                                stream=i, raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep,
+                                stream=int(g), raw=raw, tavg_istep=tavg_istep, bold=bspec, sub_istep=sim._sub_istep,
                                 stim=stim_i, aff_istep=sim._aff_istep, proj_istep=sim._proj_istep)
             specs.append(spec)
         self._specs = specs
@@ -225,4 +239,57 @@ class ParameterSweep:
                 # instances of uneven lengths give a list of (T_i, nvoi, n) arrays
                 res[key] = np.stack(arrs) if len({a.shape for a in arrs}) == 1 else arrs
         res['status'] = self.batch.status()
+        res['instances'] = self.instances.copy()
         return res
+
+
+def shard_instances(n_global, shard=None, instances=None):
+    """Global indices of the instances one process runs: all of them, the
+    rank-th of `world` contiguous balanced parts (shard=(rank, world)), or an
+    explicit list (instances=, each index once, in range)."""
+    if instances is not None:
+        idx = np.asarray(instances, dtype=np.int64).reshape(-1)
+        if idx.size and (idx.min() < 0 or idx.max() >= n_global):
+            raise IndexError('instance index out of range 0..%d' % (n_global - 1))
+        if np.unique(idx).size != idx.size:
+            raise ValueError('instance indices repeat')
+        return idx
+    if shard is None:
+        return np.arange(n_global, dtype=np.int64)
+    rank, world = (int(v) for v in shard)
+    if not 0 <= rank < world:
+        raise ValueError('shard (%d, %d): need 0 <= rank < world' % (rank, world))
+    return np.array_split(np.arange(n_global, dtype=np.int64), world)[rank]
+
+
+_PER_INSTANCE = ('raw', 'tavg', 'bold', 'sub', 'aff', 'proj', 'fc', 'status')
+
+
+def gather_sweep(res, group=None, dst=0):
+    """Collect the run() results of every rank's shard on rank `dst` and
+    reassemble them in global instance order (one gather of host objects at
+    the end of the run, over the process group's backend: NCCL between GPUs,
+    or gloo).  Returns the merged dict on `dst`, None elsewhere."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    objs = [None] * world if rank == dst else None
+    dist.gather_object(res, objs, dst=dst, group=group)
+    if rank != dst:
+        return None
+    order = np.concatenate([o['instances'] for o in objs])
+    perm = np.argsort(order, kind='stable')
+    out = {'instances': order[perm]}
+    for key in _PER_INSTANCE:
+        if key not in objs[0]:
+            continue
+        parts = [o[key] for o in objs]
+        if all(isinstance(p, np.ndarray) for p in parts) and len({p.shape[1:] for p in parts}) == 1:
+            out[key] = np.concatenate(parts)[perm]
+        else:   # uneven lengths: per-instance arrays
+            flat = [a for p in parts for a in p]
+            out[key] = [flat[k] for k in perm]
+    if 'projection' in objs[0]:
+        out['projection'] = [np.concatenate([o['projection'][m] for o in objs])[perm]
+                             for m in range(len(objs[0]['projection']))]
+    return out
