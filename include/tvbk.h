@@ -27,6 +27,8 @@
  *                          (SparseHistory.query_sparse, the delayed-state gather alone)
  *   tvbk_fc                tvb_framework/tvb/adapters/analyzers/cross_correlation_adapter.py:348-380
  *                          (numpy.corrcoef over the Bold time series, per instance)
+ *   tvbk_project           tvb_library/tvb/simulator/monitors.py:602-614
+ *                          (Projection.sample: gain.dot(state) of EEG / MEG / iEEG)
  *   tvbk_balloon           tvb_library/tvb/analyzers/fmri_balloon.py:198-364
  *                          (BalloonModel.evaluate: Balloon-Windkessel BOLD, float64)
  */
@@ -186,11 +188,7 @@ typedef struct tvbk_launch {
                                   * Linear or SigmoidalJansenRit); needs every delay >= 1 and
                                   * 1 <= sync_every <= the smallest delay.  With rings in shared memory the
                                   * kernel then stages max_ring_len + TVBK_RING_GUARD slots per instance (the
-                                  * guard slots mirror slots 0..TVBK_RING_GUARD-1).  3: as 1, and with rings in
-                                  * shared memory the straight-line blocks of four steps gather the next
-                                  * block's couplings while they advance their own; needs
-                                  * 4 <= sync_every <= the smallest delay - 3 (elsewhere it acts as 1).
-                                  * 2: the same overlap as 1 with separate
+                                  * guard slots mirror slots 0..TVBK_RING_GUARD-1).  2: the same overlap with separate
                                   * warps -- ceil(max_n / 32) gather warps sum the rows of step s + 1 while as
                                   * many update warps advance step s (rings in shared memory, row degrees
                                   * <= 64; one CTA barrier per step) */
@@ -246,7 +244,7 @@ int tvbk_sparse_layout(const double* weights, const int32_t* idelays, int32_t n,
 int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weight, int32_t nnz,
                     int32_t n, int32_t ncvar, tvbk_edge* edges);
 
-/* Slots past the end of a ring staged in shared memory with prefetch = 1 or 3:
+/* Slots past the end of a ring staged in shared memory with prefetch = 1:
  * they mirror slots 0..TVBK_RING_GUARD-1, so that the gathers of four steps
  * in a row take one ring address per edge (address + r slots, r <= 3). */
 #define TVBK_RING_GUARD 3
@@ -287,6 +285,17 @@ int tvbk_gather_delayed(const tvbk_inst* inst_host, int32_t ncvar, int64_t step,
  * (instance-major), fc is [n_inst][n][n] float64.  Rows with zero variance
  * give NaN like numpy.corrcoef. */
 int tvbk_fc(const double* x, int32_t n_inst, int32_t T, int32_t n, double* fc, void* stream);
+
+/* Sensor signals of a projection monitor from the simulation's period-mean
+ * stream (the launch's `proj` output), float64 on the device:
+ *   y[t][v][s] = sum_r gain[s][r] * x[t][voi[v]][r]
+ * x is [T][nvoi][n] float32 (the rows of several instances may be stacked
+ * into T), voi [nvoi_m] int32 (device) picks the monitor's observed
+ * variables, gain [S][n] float64 is the region lead field, y is
+ * [T][nvoi_m][S] float64.  Each output is one fma chain over r in order, so
+ * a row's value does not depend on the other rows of the launch. */
+int tvbk_project(const float* x, int64_t T, int32_t nvoi, int32_t n, const int32_t* voi, int32_t nvoi_m,
+                 const double* gain, int32_t S, double* y, void* stream);
 
 /* Balloon-Windkessel BOLD of neural-activity series, float64
  * (tvb_library/tvb/analyzers/fmri_balloon.py:198-364, BalloonModel.evaluate with the

@@ -708,6 +708,30 @@ def test_projection_monitors_vs_reference(case):
         np.testing.assert_allclose(y, y2, rtol=1e-12, atol=1e-12)
 
 
+@pytest.mark.parametrize('T,nvoi,voi,n,S', [(1, 1, [0], 1, 1), (37, 3, [2, 0], 40, 16), (300, 2, [1], 998, 65),
+                                              (129, 4, [3, 1, 0], 77, 130)])
+def test_projection_kernel_vs_numpy(T, nvoi, voi, n, S):
+    """tvbk_project (the float64 lead-field product of the projection monitors, monitors.py:602-614) against
+    numpy in float64, ragged tile edges included; each row's result does not depend on the other rows of the
+    launch (a stacked sweep gives the bits of one instance alone)."""
+    import torch
+    from tvb_b200.simulator import project_samples
+
+    class Mon:
+        pass
+    rng = np.random.default_rng(T + n + S)
+    x = rng.standard_normal((T, nvoi, n)).astype(np.float32)
+    m = Mon()
+    m.gain, m.voi = rng.standard_normal((S, n)), np.array(voi)
+    y = project_samples(torch.from_numpy(x).cuda(), m).cpu().numpy()
+    ref = np.einsum('sr,tvr->tvs', m.gain, x[:, voi].astype(np.float64))
+    assert y.shape == (T, len(voi), S)
+    np.testing.assert_allclose(y, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    k = T // 2
+    one = project_samples(torch.from_numpy(x[k:k + 1]).cuda(), m).cpu().numpy()
+    np.testing.assert_array_equal(one[0], y[k])
+
+
 def test_projection_sweep_matches_simulator():
     """ParameterSweep's EEG signals (one GEMM over all instances) equal each instance's own Simulator run."""
     from tvb_b200 import coupling, integrators, models

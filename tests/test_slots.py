@@ -52,12 +52,10 @@ def test_batch_pads_the_ring_and_keeps_two_ctas_per_sm():
                         [0.1, 0.0], 100, sigma=np.full((1, n), 0.01, np.float32))
     b = Batch(_lib.MODEL_IDS['ReducedWongWang'], _lib.CFUN_IDS['Linear'], _lib.SCHEME_IDS['EulerStochastic'],
               _lib.NOISE_PHILOX, 0.1, [0], [spec], device='cpu', allocate=False)
-    assert b.ring_in_smem and b.prefetch in (1, 3) and b.slot_width == 32
+    assert b.ring_in_smem and b.prefetch == 1 and b.slot_width == 32
     RL = b.meta[0]['ring_len']
     assert RL >= H + b.sync_every and RL * n % 32 == 0
     # the ring plus its mirrored guard slots keeps two CTAs per SM resident
     assert b.guard == _lib.RING_GUARD
     assert 228 * 1024 // ((RL + b.guard) * n * 4 + 1024) == 2
-    # the window for the one-block-ahead gather: 4 <= K <= d_min - 3
-    if b.prefetch == 3:
-        assert 4 <= b.sync_every <= c.min_delay - 3
+    assert 4 <= b.sync_every <= c.min_delay

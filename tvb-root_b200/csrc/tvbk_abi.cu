@@ -194,10 +194,7 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: voi %d out of range", L->voi[v]);
     if (L->sync_every < 1) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: sync_every must be >= 1");
     if (L->max_degree < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_degree < 0");
-    if (L->prefetch < 0 || L->prefetch > 3)
-        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch must be 0, 1, 2 or 3");
-    if (L->prefetch == 3 && L->sync_every < 4)
-        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch 3 needs sync_every >= 4");
+    if (L->prefetch < 0 || L->prefetch > 2) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch must be 0, 1 or 2");
     if (L->prefetch == 2 && (!L->ring_in_smem || L->lanes > 1 || L->edges_per_thread != 0 || L->cluster > 1 ||
                              L->cfun == TVBK_CFUN_DIFFERENCE || L->max_degree > 64 || L->model == TVBK_MODEL_SUM))
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch 2 (separate gather warps) needs rings in shared memory, "
@@ -206,7 +203,7 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
     if ((L->inst_order || L->occupancy) &&
         (L->lanes > 1 || L->cluster > 1 || L->edges_per_thread != 0 || L->prefetch == 2))
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: inst_order and occupancy apply to the row kernel (lanes 1, no "
-                    "cluster, edges_per_thread 0, prefetch 0, 1 or 3)");
+                    "cluster, edges_per_thread 0, prefetch 0 or 1)");
     if (L->max_steps < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_steps < 0");
     if (!(L->dt > 0.0f)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: dt must be > 0");
     const bool stoch = L->scheme == TVBK_SCHEME_EULER_STOCH || L->scheme == TVBK_SCHEME_HEUN_STOCH;
@@ -278,8 +275,8 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (L->max_ring_len <= 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_ring_len <= 0");
         // the row kernel stages one pre-applied sigmoid value per (slot, region) for SigmoidalJansenRit
         const int64_t ncv_g = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
-        // with prefetch 1 or 3 the row kernel keeps TVBK_RING_GUARD mirrored slots past the ring's end
-        const bool guard = (L->prefetch == 1 || L->prefetch == 3) && L->lanes <= 1;
+        // with prefetch 1 the row kernel keeps TVBK_RING_GUARD mirrored slots past the ring's end
+        const bool guard = L->prefetch == 1 && L->lanes <= 1;
         const int64_t slots = (int64_t)L->max_ring_len + (guard ? TVBK_RING_GUARD : 0);
         int64_t b = slots * L->max_n * ncv_g * (int64_t)sizeof(float);
         // separate gather warps pass the sums through a double buffer after the ring

@@ -22,7 +22,7 @@ __device__ __forceinline__ int gather_addr(int base_off, int edge_off, int ring_
 // Generic2dOscillator (tvb/simulator/models/oscillator.py:387-395).
 // params: tau, I, a, b, c, d, e, f, g, alpha, beta, gamma
 struct G2D {
-    static constexpr int NSV = 2, NCV = 1, NINT = 2, NOBS = 4, NP = 12;
+    static constexpr int NSV = 2, NCV = 1, NINT = 2, NOBS = 4, NP = 12, NPX = NP;
     __device__ static constexpr int cvar(int k) { return 0; }
     __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* x, const float* c, const float* p, float* dx) {
@@ -48,7 +48,7 @@ struct G2D {
 // JansenRit (tvb/simulator/models/jansen_rit.py:274-289); coupling enters dy4 via c[0].
 // params: A, B, a, b, v0, nu_max, r, J, a_1, a_2, a_3, a_4, mu
 struct JansenRit {
-    static constexpr int NSV = 6, NCV = 2, NINT = 6, NOBS = 6, NP = 13;
+    static constexpr int NSV = 6, NCV = 2, NINT = 6, NOBS = 6, NP = 13, NPX = NP;
     __device__ static constexpr int cvar(int k) { return k == 0 ? 1 : 2; }
     __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* y, const float* c, const float* p, float* dx) {
@@ -74,49 +74,53 @@ struct JansenRit {
     __device__ __forceinline__ static void bound(float* x) {}
 };
 
-// expm1(x) / x = sum_{k=0..12} x^k / (k+1)!, the Taylor series of expm1
-// divided by x, for |x| <= 1: the truncation (the x^13 / 14! term, below
-// 1.2e-11 relative) is far under float32 rounding.
-__device__ __forceinline__ float expm1_over_x(float x) {
-    float q = 1.0f / 6227020800.0f;  // 1 / 13!
-    q = fmaf(q, x, 1.0f / 479001600.0f);
-    q = fmaf(q, x, 1.0f / 39916800.0f);
-    q = fmaf(q, x, 1.0f / 3628800.0f);
-    q = fmaf(q, x, 1.0f / 362880.0f);
-    q = fmaf(q, x, 1.0f / 40320.0f);
-    q = fmaf(q, x, 1.0f / 5040.0f);
-    q = fmaf(q, x, 1.0f / 720.0f);
-    q = fmaf(q, x, 1.0f / 120.0f);
-    q = fmaf(q, x, 1.0f / 24.0f);
-    q = fmaf(q, x, 1.0f / 6.0f);
-    q = fmaf(q, x, 0.5f);
-    return fmaf(q, x, 1.0f);
+// z / (1 - exp(-z)) for |z| <= 1 from its Bernoulli-number series,
+//   z / (1 - e^-z) = 1 + z/2 + sum_k B_2k z^2k / (2k)!
+//                  = 1 + z/2 + z^2/12 - z^4/720 + z^6/30240 - z^8/1209600 + z^10/47900160 - ...
+// (B_2 = 1/6, B_4 = -1/30, B_6 = 1/42, B_8 = -1/30, B_10 = 5/66).  Truncated
+// after z^10: the rest is below 9e-10 relative on |z| <= 1, far under float32
+// rounding.  Even powers only, so the polynomial runs in w = z^2: five
+// dependent fmas instead of the thirteen of a Taylor series in z.
+__device__ __forceinline__ float z_over_one_minus_exp(float z) {
+    const float w = z * z;
+    float q = 1.0f / 47900160.0f;
+    q = fmaf(q, w, -1.0f / 1209600.0f);
+    q = fmaf(q, w, 1.0f / 30240.0f);
+    q = fmaf(q, w, -1.0f / 720.0f);
+    q = fmaf(q, w, 1.0f / 12.0f);
+    return fmaf(w, q, fmaf(z, 0.5f, 1.0f));
 }
 
 // ReducedWongWang (tvb/simulator/models/wong_wang.py:36-42); S bounded to [0, 1] (wong_wang.py:129-133).
-// params: a, b, d, gamma, tau_s, w, J_N, I_o (prepare() replaces tau_s by 1 / tau_s)
+// params: a, b, d, gamma, tau_s, w, J_N, I_o; prepare() replaces tau_s by 1 / tau_s and appends
+// 1 / d and w J_N (NPX = 10 kernel-side values)
 //
-// H(x) = (a x - b) / (1 - exp(-d (a x - b))) = -y / expm1(-d y) with
-// y = a x - b.  For |d y| <= 1 it is 1 / (d * (expm1(-d y) / (-d y))), the
-// ratio from its series: no cancellation near y = 0 and no 0/0 at y = 0 (the
-// limit 1/d comes out of the same expression); for |d y| > 1, where
-// exp(-d y) - 1 does not cancel, -y / (exp(-d y) - 1) with the hardware
-// exponential.  Both forms are evaluated and one is selected (no branch).
+// H(x) = (a x - b) / (1 - exp(-d (a x - b))) = y / (1 - exp(-z)) with
+// y = a x - b, z = d y.  For |z| <= 1 it is (1 / d) * z / (1 - exp(-z)),
+// the series above: no cancellation near y = 0 and no 0/0 at y = 0 (the
+// limit 1/d comes out of the same expression); for |z| > 1, where
+// 1 - exp(-z) does not cancel, y / (1 - exp(-z)) with the hardware
+// exponential and reciprocal (__fdividef: for z -> -inf the denominator
+// overflows to -inf and H to the limit 0).  Both forms are evaluated and one
+// is selected (no branch).
 struct RWW {
-    static constexpr int NSV = 1, NCV = 1, NINT = 1, NOBS = 1, NP = 8;
+    static constexpr int NSV = 1, NCV = 1, NINT = 1, NOBS = 1, NP = 8, NPX = 10;
     __device__ static constexpr int cvar(int k) { return 0; }
-    __device__ __forceinline__ static void prepare(float* p) { p[4] = 1.0f / p[4]; }
+    __device__ __forceinline__ static void prepare(float* p) {
+        p[4] = 1.0f / p[4];
+        p[8] = 1.0f / p[2];
+        p[9] = p[5] * p[6];
+    }
     __device__ __forceinline__ static void dfun(const float* x, const float* c, const float* p, float* dx) {
         const float S = x[0];
-        const float a = p[0], b = p[1], d = p[2], gamma = p[3], inv_tau_s = p[4], w = p[5], JN = p[6], Io = p[7];
-        const float xx = w * JN * S + Io + JN * c[0];
+        const float a = p[0], b = p[1], d = p[2], gamma = p[3], inv_tau_s = p[4], JN = p[6], Io = p[7];
+        const float inv_d = p[8], wJN = p[9];
+        const float xx = wJN * S + Io + JN * c[0];
         const float y = a * xx - b;
-        const float dy = d * y;
-        const bool small = fabsf(dy) <= 1.0f;
-        const float q = expm1_over_x(small ? -dy : 0.0f);
-        const float num = small ? 1.0f : -y;
-        const float den = small ? d * q : __expf(-dy) - 1.0f;
-        const float h = num * __frcp_rn(den);
+        const float z = d * y;
+        const float h_small = z_over_one_minus_exp(z) * inv_d;
+        const float h_large = __fdividef(y, 1.0f - __expf(-z));
+        const float h = fabsf(z) <= 1.0f ? h_small : h_large;
         dx[0] = fmaf((1.0f - S) * h, gamma, -(S * inv_tau_s));
     }
     __device__ __forceinline__ static float observe(int k, const float* x) { return x[0]; }
@@ -126,7 +130,7 @@ struct RWW {
 // Epileptor (tvb/simulator/models/epileptor.py:36-71).
 // params: a, b, c, d, r, x0, Iext, slope, Iext2, tau, aa, bb, Kvf, Kf, Ks, tt, modification
 struct Epileptor {
-    static constexpr int NSV = 6, NCV = 2, NINT = 6, NOBS = 7, NP = 17;
+    static constexpr int NSV = 6, NCV = 2, NINT = 6, NOBS = 7, NP = 17, NPX = NP;
     __device__ static constexpr int cvar(int k) { return k == 0 ? 0 : 3; }
     __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* y, const float* c, const float* p, float* dx) {
@@ -172,7 +176,7 @@ struct Epileptor {
 // dx = x + c: the model of the reference's exact-propagation test
 // (tvb/tests/library/simulator/history_test.py), used with the Identity scheme.
 struct SumModel {
-    static constexpr int NSV = 1, NCV = 1, NINT = 1, NOBS = 1, NP = 1;
+    static constexpr int NSV = 1, NCV = 1, NINT = 1, NOBS = 1, NP = 1, NPX = NP;
     __device__ static constexpr int cvar(int k) { return 0; }
     __device__ __forceinline__ static void prepare(float* p) {}
     __device__ __forceinline__ static void dfun(const float* x, const float* c, const float* p, float* dx) {

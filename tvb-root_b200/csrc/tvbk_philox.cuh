@@ -29,8 +29,10 @@ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
     const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
-        const uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+        // each 32 x 32 -> 64-bit product in one wide multiply (high and low halves together)
+        const uint64_t p0 = (uint64_t)M0 * c0, p1 = (uint64_t)M1 * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
         const uint32_t n0 = hi1 ^ c1 ^ k0;
         const uint32_t n2 = hi0 ^ c3 ^ k1;
         c0 = n0;
@@ -48,8 +50,12 @@ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint3
     return out;
 }
 
+// (m + 1/2) 2^-23 with m = x >> 9 < 2^23, built from the bits: 1 + m 2^-23 is
+// the float with exponent 0 and mantissa m, and subtracting 1 - 2^-24 from
+// it is exact (Sterbenz), giving (2m + 1) 2^-24 -- the same value as
+// (float(m) + 0.5) * 2^-23, without the integer-to-float conversion.
 __device__ __forceinline__ float uniform_open(uint32_t x) {
-    return (__uint2float_rn(x >> 9) + 0.5f) * 1.1920928955078125e-07f;  // 2^-23
+    return __uint_as_float((x >> 9) | 0x3f800000u) - 0.99999994039535522461f;  // 1 - 2^-24
 }
 
 // Box-Muller: r = sqrt(-2 ln u1); (r cos 2 pi u2, r sin 2 pi u2), with the
@@ -63,10 +69,10 @@ __device__ __forceinline__ float uniform_open(uint32_t x) {
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
     const float u1 = uniform_open(a);
     const float u2 = uniform_open(b);
-    const float r2 = -2.0f * __logf(u1);
+    const float r2 = __log2f(u1) * -1.38629436111989061883f;  // -2 ln u1 = log2(u1) * (-2 ln 2)
     const float r = r2 * rsqrtf(r2);
     float s, c;
-    __sincosf(3.14159265358979f * fmaf(2.0f, u2, -1.0f), &s, &c);
+    __sincosf(fmaf(6.28318530717958647693f, u2, -3.14159265358979323846f), &s, &c);  // pi (2 u2 - 1)
     z0 = -r * c;
     z1 = -r * s;
 }

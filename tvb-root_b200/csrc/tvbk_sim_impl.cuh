@@ -321,7 +321,8 @@ struct Node {
     static constexpr bool STOCH = SchemeTraits<SCHEME>::stoch;
     static constexpr int MV = M::NOBS < TVBK_MAX_VOI ? M::NOBS : TVBK_MAX_VOI;  // nvoi <= nobs checked on the host
 
-    float x[NSV], p[NP], sig[NINT], zc[NINT][4], tacc[MV];
+    // p: the NP parameters of the region, then the NPX - NP values M::prepare() derives from them
+    float x[NSV], p[M::NPX], sig[NINT], zc[NINT][4], tacc[MV];
     double bacc[MV];
     float* raw_p;
     const float* fed_p;
@@ -840,7 +841,7 @@ __device__ __forceinline__ void stage_ring(float* dst, const float* src, int nfl
 // barrier interval K <= d_min, and a coupling whose pre() ignores x_i.
 // EXT = false: no region stimulus and no AfferentCoupling monitor (launch.extras
 // == 0); an instance that asks for either gets TVBK_STATUS_UNSUPPORTED.
-template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE, bool EXT = true, bool AHEAD = false>
+template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE, bool EXT = true>
 __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     constexpr int NCV = M::NCV;
     constexpr bool SIGMA = GatherTraits<CF, NCV>::SIGMA;
@@ -873,7 +874,6 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
     // couple4 read up to three slots past a wrapped address); every write of
     // one of those slots also goes to its mirror.
     constexpr bool GUARDED = SMEM && PIPE && MAXD > 0;
-    static_assert(!AHEAD || GUARDED, "the one-block-ahead gather reads guarded shared-memory rings");
     constexpr int GUARD = GUARDED ? TVBK_RING_GUARD : 0;
     if constexpr (SIGMA) {
         sigma_ring(ring, Ip->ring, RL * n, threadIdx.x, blockDim.x, cf);
@@ -959,12 +959,6 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
         int64_t zq = -1;  // Philox block whose normals are in node.zc
         float cnext[NCV];
         if (act) row.couple(ring, wslot * slot_floats, ring_floats, node.x, cf, cnext);
-        // AHEAD: cq holds the couplings of the four steps from ks = cq_k on, gathered by the previous
-        // straight-line block (cq_k = -1: none)
-        float cq[4][NCV];
-        int cq_k = -1;
-        (void)cq;
-        (void)cq_k;
         int64_t s = s0 + 1;  // the step to do next
         int ks = 0;
         while (ks < nsteps) {
@@ -990,17 +984,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                         // four gathers are independent of the block's updates and of each other
                         float cb[4][NCV];
                         (void)cb;
-                        if constexpr (AHEAD) {
-                            // one block ahead: the couplings of steps s + 4 .. s + 7 (times s + 3 - d ..
-                            // s + 6 - d <= s - 1, since d >= d_min >= K + 3), gathered while this block's
-                            // four updates run on the couplings gathered by the previous block
-                            if (cq_k != ks) {  // the first straight-line block after one-step steps
-                                row.couple4(ring, wslot * slot_floats, ring_floats, slot_floats, cf, cq);
-                            }
-                            int a_slot = wslot + 4;  // slot of time s + 3
-                            a_slot = a_slot >= RL ? a_slot - RL : a_slot;
-                            row.couple4(ring, a_slot * slot_floats, ring_floats, slot_floats, cf, cb);
-                        } else if constexpr (GUARDED) {
+                        if constexpr (GUARDED) {
                             const int s0slot = (wslot + 1 == RL) ? 0 : wslot + 1;  // slot of time s
                             row.couple4(ring, s0slot * slot_floats, ring_floats, slot_floats, cf, cb);
                         }
@@ -1010,13 +994,7 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
 #pragma unroll
                             for (int k = 0; k < NCV; ++k) c[k] = cnext[k];
                             wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s + r
-                            if constexpr (AHEAD) {
-#pragma unroll
-                                for (int k = 0; k < NCV; ++k) {
-                                    c[k] = cq[r][k];
-                                    cnext[k] = r < 3 ? cq[r + 1][k] : cb[0][k];
-                                }
-                            } else if constexpr (GUARDED) {
+                            if constexpr (GUARDED) {
 #pragma unroll
                                 for (int k = 0; k < NCV; ++k) cnext[k] = cb[r][k];
                             } else {
@@ -1040,12 +1018,6 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
 #pragma unroll
                                 for (int r = 0; r < 4; ++r) node.zc[k][r] = zn[k][r];
                         }
-                        if constexpr (AHEAD) {
-#pragma unroll
-                            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                                for (int k = 0; k < NCV; ++k) cq[r][k] = cb[r][k];
-                        }
                     } else {
 #pragma unroll
                         for (int r = 0; r < 4; ++r) {
@@ -1066,7 +1038,6 @@ __global__ void __launch_bounds__(MAXT) sim_kernel(const tvbk_launch L) {
                 since_sync += 4;
                 s += 4;
                 ks += 4;
-                cq_k = ks;
             } else {
                 wslot = (wslot + 1 == RL) ? 0 : wslot + 1;  // time s
                 if (act) {
@@ -1245,10 +1216,9 @@ __global__ void __launch_bounds__(512) sim_kernel_ep(const tvbk_launch L) {
 
 // ------------------------------------------------------------------ launch
 
-template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE = false, bool EXT = true,
-          bool AHEAD = false>
+template <class M, int CF, int SCHEME, bool SMEM, int MAXT, int MAXD, bool PIPE = false, bool EXT = true>
 int launch_one(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes) {
-    auto kern = sim_kernel<M, CF, SCHEME, SMEM, MAXT, MAXD, PIPE, EXT, AHEAD>;
+    auto kern = sim_kernel<M, CF, SCHEME, SMEM, MAXT, MAXD, PIPE, EXT>;
     if (smem_bytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
         if (e != cudaSuccess) return (int)e;
@@ -1272,13 +1242,6 @@ int launch_deg(const tvbk_launch& L, cudaStream_t st, size_t smem_bytes, int max
         if (L.prefetch) {
             // rings in shared memory without stimulus or AfferentCoupling: the lean build
             if (SMEM && L.extras == 0) {
-                // prefetch 3: the straight-line blocks gather one block ahead (4 <= K <= d_min - 3)
-                if (L.prefetch == 3) {
-                    if (max_deg <= 32)
-                        return launch_one<M, CF, SCHEME, SMEM, MAXT, 32, true, false, SMEM>(L, st, smem_bytes);
-                    if (max_deg <= 64)
-                        return launch_one<M, CF, SCHEME, SMEM, MAXT, 64, true, false, SMEM>(L, st, smem_bytes);
-                }
                 if (max_deg <= 32) return launch_one<M, CF, SCHEME, SMEM, MAXT, 32, true, false>(L, st, smem_bytes);
                 if (max_deg <= 64) return launch_one<M, CF, SCHEME, SMEM, MAXT, 64, true, false>(L, st, smem_bytes);
             }

@@ -32,7 +32,7 @@ NOISE_NONE, NOISE_FED, NOISE_PHILOX = 0, 1, 2
 MAX_REGIONS = 1024
 MAX_VOI = 8
 STATIC_SCRATCH_BYTES = 8 * 1024 * 1024
-# mirrored slots past the end of a ring staged in shared memory with prefetch = 1 or 3 (TVBK_RING_GUARD)
+# mirrored slots past the end of a ring staged in shared memory with prefetch = 1 (TVBK_RING_GUARD)
 RING_GUARD = 3
 
 
@@ -145,6 +145,7 @@ _SIGNATURES = {
     'tvbk_sim_run': (_I32, [ctypes.POINTER(Launch), _P]),
     'tvbk_gather_delayed': (_I32, [ctypes.POINTER(Inst), _I32, _I64, _P, _P]),
     'tvbk_fc': (_I32, [_P, _I32, _I32, _I32, _P, _P]),
+    'tvbk_project': (_I32, [_P, _I64, _I32, _I32, _P, _I32, _P, _I32, _P, _P]),
     'tvbk_balloon': (_I32, [_P, _I32, _I64, _D, _P, _I32, _P, _P]),
     'tvbk_sim_run_static': (_I32, [ctypes.POINTER(Launch), ctypes.POINTER(Inst), _P, _P]),
 }

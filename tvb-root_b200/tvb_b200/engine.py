@@ -297,10 +297,6 @@ class Batch:
             # row kernel with the next step's gather issued ahead: barrier interval K <= d_min
             self.prefetch = 1
             self.sync_every = min(self.sync_every, dmin)
-            if self.ring_in_smem and V == 1 and gather != 'split' and dmin >= 7 and self.sync_every >= 4:
-                # the straight-line blocks also gather one block of four steps ahead: K <= d_min - 3
-                self.prefetch = 3
-                self.sync_every = min(self.sync_every, dmin - 3)
         if gather == 'split':
             # separate gather and update warps (the prefetch overlap across warps)
             ring_b = -(-(hmax + self.sync_every) * self.max_n * self.ncvar_gather * 4 // 16) * 16
@@ -315,8 +311,8 @@ class Batch:
                 self.edges_per_thread, self.block_threads, self.sync_every = ep
             elif gather == 'edge':
                 raise ValueError('the edge-parallel gather does not apply to this batch')
-        # mirrored guard slots past a shared-memory ring (prefetch 1 or 3; the split kernel has none)
-        self.guard = _lib.RING_GUARD if (self.prefetch in (1, 3) and self.ring_in_smem and V == 1) else 0
+        # mirrored guard slots past a shared-memory ring (prefetch 1; the split kernel has none)
+        self.guard = _lib.RING_GUARD if (self.prefetch == 1 and self.ring_in_smem and V == 1) else 0
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
         self.slot_width, self._ring_len = self._choose_slots()
         self._plan()

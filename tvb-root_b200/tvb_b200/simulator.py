@@ -129,12 +129,21 @@ def adopt_connectivity(conn):
 
 def project_samples(proj, m):
     """(T, nvoi_m, S) = gain . mean for the device stream proj (T, nvoi, n)
-    float32 of window means and projection monitor m: a float64 GEMM on the
-    device over all samples at once."""
+    float32 of window means and projection monitor m: the library's float64
+    projection kernel (tvbk_project) over all samples at once."""
+    import ctypes
     import torch
-    g = torch.as_tensor(m.gain, dtype=torch.float64, device=proj.device)          # (S, n)
-    x = proj[:, torch.as_tensor(np.asarray(m.voi), device=proj.device)].to(torch.float64)
-    return torch.matmul(x, g.T)
+    proj = proj.contiguous()
+    T, nvoi, n = proj.shape
+    g = torch.as_tensor(np.ascontiguousarray(m.gain, dtype=np.float64), device=proj.device)   # (S, n)
+    voi = torch.as_tensor(np.asarray(m.voi, dtype=np.int32).reshape(-1), device=proj.device)
+    S = g.shape[0]
+    y = torch.empty((T, voi.numel(), S), dtype=torch.float64, device=proj.device)
+    st = torch.cuda.current_stream(proj.device)
+    _lib.check(_lib.load().tvbk_project(ctypes.c_void_p(proj.data_ptr()), T, nvoi, n, ctypes.c_void_p(voi.data_ptr()),
+                                        voi.numel(), ctypes.c_void_p(g.data_ptr()), S, ctypes.c_void_p(y.data_ptr()),
+                                        ctypes.c_void_p(st.cuda_stream)), 'tvbk_project')
+    return y
 
 
 def noise_sigma(nsig, nintvar, n, dt):
