@@ -228,6 +228,72 @@ def case_g2d(R):
          ref_seconds=res['stock']['el'])
 
 
+def case_g2d_full(R):
+    """The plain method at its stated length: Generic2dOscillator, 76 regions,
+    Linear a=0.0152, HeunDeterministic dt 0.1, Raw + TemporalAverage(1 ms),
+    1000 ms (10 000 steps).  Keeps the TemporalAverage and every 10th Raw row
+    (stock and all-float64)."""
+    w, L = synthetic_connectome(76, 0.40, 10.0, 200.0, seed=1)
+    speed, dt, length = 3.0, 0.1, 1000.0
+
+    def build():
+        return R['simulator'].Simulator(
+            model=R['models'].Generic2dOscillator(),
+            connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].Linear(a=np.array([0.0152])),
+            integrator=R['integrators'].HeunDeterministic(dt=dt),
+            monitors=[R['monitors'].Raw(), R['monitors'].TemporalAverage(period=1.0)],
+            simulation_length=length)
+    res = {}
+    for var in ('stock', 'fp64'):
+        sim, cfg, out, _, el = run_sim(R, build, length, var == 'fp64', ic_seed=101)
+        (tr, raw), (tt, tavg) = out
+        res[var] = dict(cfg=cfg, raw=raw[9::10, ..., 0], raw_t=tr[9::10], tavg=tavg[..., 0], tavg_t=tt, el=el)
+    c = res['stock']['cfg']
+    save('g2d_76_full', weights=w, tract_lengths=L, speed=speed, dt=dt, length=length,
+         conn_recipe=np.array([76, 0.40, 10.0, 200.0, 1]), ic_seed=101, coupling_a=0.0152, **c,
+         raw_every10=res['stock']['raw'], raw_every10_t=res['stock']['raw_t'],
+         raw_every10_fp64=res['fp64']['raw'],
+         tavg=res['stock']['tavg'], tavg_t=res['stock']['tavg_t'], tavg_fp64=res['fp64']['tavg'],
+         ref_seconds=res['stock']['el'])
+
+
+def case_epi_stats(R, k, length=2000.0):
+    """Instance k of the large-network batch (Epileptor, 998 regions, 10 %
+    density, tract lengths 5-300 mm, speed 3 mm/ms, x0 row k of
+    default_rng(14).uniform(-2.4, -1.6, (16, 998)), Difference coupling,
+    HeunDeterministic dt 0.05, TemporalAverage(1 ms), initial history drawn
+    after numpy.random.seed(15)) over `length` ms.  The trajectory is chaotic
+    beyond a few tens of ms, so the fixture keeps statistics over the whole
+    run -- per-region mean and variance of each observed variable -- and the
+    TemporalAverage of 32 regions (for their FC), for the stock and the
+    all-float64 reference."""
+    w, L = synthetic_connectome(998, 0.10, 5.0, 300.0, seed=4)
+    x0 = np.random.default_rng(14).uniform(-2.4, -1.6, (16, 998))[k]
+    speed, dt = 3.0, 0.05
+    pick = np.linspace(0, 997, 32).round().astype(int)
+
+    def build():
+        return R['simulator'].Simulator(
+            model=R['models'].Epileptor(x0=x0.copy()), connectivity=make_conn(R, w, L, speed),
+            coupling=R['coupling'].Difference(), integrator=R['integrators'].HeunDeterministic(dt=dt),
+            monitors=[R['monitors'].TemporalAverage(period=1.0)], simulation_length=length)
+    res = {}
+    for var in ('stock', 'fp64'):
+        sim, cfg, out, _, el = run_sim(R, build, length, var == 'fp64', ic_seed=15)
+        print('epi_stats', k, var, '%.1fs' % el, flush=True)
+        (tt, tavg), = out
+        y = tavg[..., 0]
+        res[var] = dict(cfg=cfg, mean=y.mean(axis=0), var=y.var(axis=0), sub=y[:, 0, pick], t=tt, el=el)
+    c = res['stock']['cfg']
+    save('epi_998_stats_%d' % k, conn_recipe=np.array([998, 0.10, 5.0, 300.0, 4]), speed=speed, dt=dt,
+         length=length, x0=x0, ic_seed=15, instance=k, pick=pick, idelays=c['idelays'],
+         buffer0=c['buffer0'], state0=c['state0'], tavg_t=res['stock']['t'],
+         mean=res['stock']['mean'], var=res['stock']['var'], sub=res['stock']['sub'],
+         mean_fp64=res['fp64']['mean'], var_fp64=res['fp64']['var'], sub_fp64=res['fp64']['sub'],
+         ref_seconds=res['stock']['el'])
+
+
 def case_jr(R, length=4000.0):
     """JansenRit, 192 regions, SigmoidalJansenRit, HeunStochastic dt 0.05 with
     additive nsig 1e-5 on y4 only, TemporalAverage(1 ms) + Bold(2000 ms)."""
@@ -767,6 +833,9 @@ def main():
         'idelays': lambda: case_idelays(R),
         'difference': lambda: case_difference(R),
         'g2d': lambda: case_g2d(R),
+        'g2d_full': lambda: case_g2d_full(R),
+        'epi_stats_0': lambda: case_epi_stats(R, 0),
+        'epi_stats_1': lambda: case_epi_stats(R, 1),
         'epi': lambda: case_epi(R, 'epi_998', 998, 0.10, 60.0, {}, seed=4),
         'epi_coupled': lambda: case_epi(R, 'epi_96_coupled', 96, 0.3, 200.0,
                                         {'Ks': -0.2, 'Kf': 0.05, 'Kvf': 0.02}, seed=14),

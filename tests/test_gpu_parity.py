@@ -134,6 +134,35 @@ def test_g2d_76_linear_heun_raw_tavg():
     report('g2d raw vs all-fp64 reference', raw[..., 0], fx['raw_fp64'], 1e-4)
 
 
+def test_g2d_76_full_length_1000ms():
+    """The plain method at its stated length (10 000 steps): TemporalAverage and every 10th Raw row against
+    the stock and the all-float64 reference over the whole run.  G2D with this coupling is not chaotic, so the
+    float32 trajectory stays within a few 1e-6 of the float64 one throughout."""
+    T = tvb()
+    fx = G.load('g2d_76_full')
+    w, L = G.connectome(fx)
+    np.random.seed(int(fx['ic_seed']))
+    sim = T['Simulator'](model=T['models'].Generic2dOscillator(),
+                         connectivity=T['Connectivity'](weights=w, tract_lengths=L, speed=float(fx['speed'])),
+                         coupling=T['coupling'].Linear(a=float(fx['coupling_a'])),
+                         integrator=T['integrators'].HeunDeterministic(dt=float(fx['dt'])),
+                         monitors=[T['monitors'].Raw(), T['monitors'].TemporalAverage(period=1.0)],
+                         simulation_length=float(fx['length'])).configure()
+    np.testing.assert_array_equal(sim.history_buffer[..., 0], fx['buffer0'])
+    (tr, raw), (tt, tavg) = sim.run()
+    assert tavg.shape[0] == 1000 and raw.shape[0] == 10000
+    np.testing.assert_allclose(tt, fx['tavg_t'], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(tr[9::10], fx['raw_every10_t'], rtol=0, atol=1e-12)
+    report('g2d 1000 ms tavg vs reference', tavg[..., 0], fx['tavg'], 2e-5)
+    report('g2d 1000 ms tavg vs all-fp64 reference', tavg[..., 0], fx['tavg_fp64'], 2e-5)
+    report('g2d 1000 ms raw (every 10th) vs reference', raw[9::10, ..., 0], fx['raw_every10'], 2e-5)
+    # the error does not grow over the run: the last 100 ms hold as tightly as the first
+    late = rel_err(tavg[900:, ..., 0], fx['tavg_fp64'][900:])[0]
+    early = rel_err(tavg[:100, ..., 0], fx['tavg_fp64'][:100])[0]
+    print('g2d error first 100 ms %.2e, last 100 ms %.2e' % (early, late))
+    assert late <= 2e-5
+
+
 def _epileptor(fx, n, gains):
     T = tvb()
     w, L = G.connectome(fx)
@@ -159,8 +188,10 @@ def test_epileptor_96_difference_coupled():
     np.testing.assert_allclose(tt, fx['tavg_t'], rtol=0, atol=1e-12)
     report('epileptor 96 coupled tavg 0-20 ms', tavg[:20, ..., 0], fx['tavg'][:20], 1e-4)
     mx, rms = rel_err(tavg[..., 0], fx['tavg'])
-    print('epileptor 96 coupled tavg 0-200 ms       max_rel %.3e  rms_rel %.3e (rms bound 5e-2)' % (mx, rms))
-    assert rms <= 5e-2
+    # measured 9.1e-3; the reference's own stock and all-float64 runs differ by 2.3e-5 RMS here, and a 1e-7
+    # change of the initial state moves the float64 run by 2.6 %
+    print('epileptor 96 coupled tavg 0-200 ms       max_rel %.3e  rms_rel %.3e (rms bound 2e-2)' % (mx, rms))
+    assert rms <= 2e-2
 
 
 def test_epileptor_998_difference():
@@ -170,8 +201,8 @@ def test_epileptor_998_difference():
     (tt, tavg), = sim.run()
     report('epileptor 998 tavg 0-20 ms', tavg[:20, ..., 0], fx['tavg'][:20], 1e-4)
     mx, rms = rel_err(tavg[..., 0], fx['tavg'])
-    print('epileptor 998 tavg 0-60 ms               max_rel %.3e  rms_rel %.3e (rms bound 1e-2)' % (mx, rms))
-    assert rms <= 1e-2
+    print('epileptor 998 tavg 0-60 ms               max_rel %.3e  rms_rel %.3e (rms bound 5e-4)' % (mx, rms))
+    assert rms <= 5e-4   # measured 8.6e-5
 
 
 def test_epileptor_998_batch_uneven_lengths():
@@ -223,8 +254,8 @@ def test_jansen_rit_sigmoidal_heun_stochastic_reference_noise():
     np.testing.assert_allclose(tt[idx], fx['tavg_t'], rtol=0, atol=1e-9)
     np.testing.assert_allclose(tb, fx['bold_t'], rtol=0, atol=1e-9)
     report('jr tavg (200 ms) vs reference', tavg[idx[:10], ..., 0], fx['tavg'][:10], 1e-3)
-    report('jr tavg (4 s) vs reference', tavg[idx, ..., 0], fx['tavg'], 2e-2)
-    report('jr bold vs reference', bold[..., 0], fx['bold'], 2e-2)
+    report('jr tavg (4 s) vs reference', tavg[idx, ..., 0], fx['tavg'], 1e-3)   # measured 1.7e-4
+    report('jr bold vs reference', bold[..., 0], fx['bold'], 1e-3)              # measured 3.4e-4
 
 
 def _rww_sim(fx, k, length, noise_source='reference'):
@@ -249,18 +280,18 @@ def test_rww_68_short_reference_noise(k):
     (tb, bold), (tt, tavg) = sim.run()
     np.testing.assert_allclose(tb, fx['bold_t'], rtol=0, atol=1e-9)
     report('rww[%d] bold vs reference' % k, bold[..., 0], fx['bold_%d' % k], 1e-4)
-    report('rww[%d] tavg vs reference' % k, tavg[..., 0], fx['tavg_%d' % k], 1e-3)
+    report('rww[%d] tavg vs reference' % k, tavg[..., 0], fx['tavg_%d' % k], 2e-5)   # measured <= 1.9e-6
 
 
 @pytest.mark.parametrize('k', [0, 1])
 def test_rww_68_full_60s_bold_fc(k):
     """60 s of RWW with the reference's noise: Bold and FC (Pearson over the 30
-    Bold samples) within 1e-3 of the reference."""
+    Bold samples) within 1e-3 of the reference (the stated FC tolerance; measured <= 1.6e-6)."""
     from tvb_b200.engine import functional_connectivity
     fx = G.load('rww_68_full')
     sim = _rww_sim(fx, k, float(fx['length']))
     (tb, bold), = sim.run()
-    report('rww full[%d] bold vs reference' % k, bold[..., 0], fx['bold_%d' % k], 1e-3)
+    report('rww full[%d] bold vs reference' % k, bold[..., 0], fx['bold_%d' % k], 2e-5)   # measured <= 6.4e-7
     fc = functional_connectivity(bold[:, 0, :, 0]).cpu().numpy()[0]
     d = np.abs(fc - fx['fc_%d' % k]).max()
     d64 = np.abs(fc - fx['fc_fp64_%d' % k]).max()
@@ -319,7 +350,7 @@ def test_philox_jansen_rit_partial_noise_matches_oracle(dt):
     z = O.philox_normals(7, 0, np.arange(1, n_steps + 1), 6, 68)
     out, _ = O.simulate('JansenRit', {}, w, L, 5.0, dt, 'SigmoidalJansenRit', {}, 'HeunStochastic', n_steps,
                         [O.Monitor('TemporalAverage', 1.0)], buf0, st0, 0, nsig=nsig, noise_z=z)
-    report('philox jr (noise on y4) dt %g tavg vs oracle' % dt, tavg[..., 0], out[0][1], 1e-3)
+    report('philox jr (noise on y4) dt %g tavg vs oracle' % dt, tavg[..., 0], out[0][1], 2e-5)   # measured <= 1.9e-6
 
 
 @pytest.mark.parametrize('cfun', ['Linear', 'SigmoidalJansenRit', 'Difference'])
