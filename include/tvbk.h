@@ -182,7 +182,13 @@ typedef struct tvbk_launch {
     int32_t edges_per_thread;    /* 0: one thread per row; 8, 12, 16 or 24: edge-parallel gather with that many
                                   * register slots per thread (rings in shared memory, Linear or
                                   * SigmoidalJansenRit only; ceil(nnz / block_threads) must not exceed it nor
-                                  * the smallest non-zero row degree of any instance) */
+                                  * the smallest non-zero row degree of any instance).  With cluster > 1: 0 (a
+                                  * warp per row) or 8, 16, 32: edge runs -- each cluster CTA's edges, staged in
+                                  * shared memory (cluster_edges), cut into runs of that many edges, one per
+                                  * gather thread; it must not exceed the smallest non-zero row degree of a
+                                  * CTA's rows and the runs must cover the CTA's edges (512 threads, less one
+                                  * warp per 32 rows with prefetch); Difference is then summed as
+                                  * sum w x_j - x_i sum w and may prefetch */
     int32_t block_threads;       /* CTA size for the edge-parallel gather (multiple of 32, >= max_n, <= 512) */
     int32_t prefetch;            /* 1: issue the gather of step s + 1 before the update of step s (row kernel,
                                   * Linear or SigmoidalJansenRit); needs every delay >= 1 and

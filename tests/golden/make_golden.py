@@ -267,7 +267,8 @@ def case_epi_stats(R, k, length=2000.0):
     beyond a few tens of ms, so the fixture keeps statistics over the whole
     run -- per-region mean and variance of each observed variable -- and the
     TemporalAverage of 32 regions (for their FC), for the stock and the
-    all-float64 reference."""
+    all-float64 reference, and for the stock reference started from a current
+    state changed by 1e-7 relative (the natural scale of the divergence)."""
     w, L = synthetic_connectome(998, 0.10, 5.0, 300.0, seed=4)
     x0 = np.random.default_rng(14).uniform(-2.4, -1.6, (16, 998))[k]
     speed, dt = 3.0, 0.05
@@ -279,8 +280,20 @@ def case_epi_stats(R, k, length=2000.0):
             coupling=R['coupling'].Difference(), integrator=R['integrators'].HeunDeterministic(dt=dt),
             monitors=[R['monitors'].TemporalAverage(period=1.0)], simulation_length=length)
     res = {}
-    for var in ('stock', 'fp64'):
-        sim, cfg, out, _, el = run_sim(R, build, length, var == 'fp64', ic_seed=15)
+    for var in ('stock', 'fp64', 'perturbed'):
+        if var == 'perturbed':
+            # the scale of chaotic divergence: the stock run from a current state changed by 1e-7 relative
+            set_history_dtype(R, 'f')
+            sim = build()
+            np.random.seed(15)
+            sim.configure()
+            sim.current_state = sim.current_state * (1.0 + 1e-7)
+            t0 = time.time()
+            out = sim.run(simulation_length=length)
+            el = time.time() - t0
+            cfg = None
+        else:
+            sim, cfg, out, _, el = run_sim(R, build, length, var == 'fp64', ic_seed=15)
         print('epi_stats', k, var, '%.1fs' % el, flush=True)
         (tt, tavg), = out
         y = tavg[..., 0]
@@ -291,7 +304,8 @@ def case_epi_stats(R, k, length=2000.0):
          buffer0=c['buffer0'], state0=c['state0'], tavg_t=res['stock']['t'],
          mean=res['stock']['mean'], var=res['stock']['var'], sub=res['stock']['sub'],
          mean_fp64=res['fp64']['mean'], var_fp64=res['fp64']['var'], sub_fp64=res['fp64']['sub'],
-         ref_seconds=res['stock']['el'])
+         mean_perturbed=res['perturbed']['mean'], var_perturbed=res['perturbed']['var'],
+         sub_perturbed=res['perturbed']['sub'], ref_seconds=res['stock']['el'])
 
 
 def case_jr(R, length=4000.0):

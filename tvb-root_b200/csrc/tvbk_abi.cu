@@ -219,9 +219,16 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
     if (L->cluster < 0 || L->cluster > 16)
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster %d out of 0..16", L->cluster);
     if (L->cluster > 1) {
-        if (L->lanes > 1 || L->edges_per_thread != 0 || L->ring_in_smem)
-            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster per instance uses the row gather with rings in "
-                        "place (lanes 1, edges_per_thread 0, ring_in_smem 0)");
+        if (L->lanes > 1 || L->ring_in_smem)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster per instance reads its rings in place "
+                        "(lanes 1, ring_in_smem 0)");
+        const int E = L->edges_per_thread;
+        if (E != 0 && E != 8 && E != 16 && E != 32)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster's edge runs have 8, 16 or 32 edges (or 0: a warp "
+                        "per row)");
+        if (E == 0 && L->prefetch && L->cfun == TVBK_CFUN_DIFFERENCE)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster with a warp per row cannot prefetch Difference "
+                        "coupling (use edge runs)");
         if (L->model == TVBK_MODEL_SUM) return fail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run: clusters with the Sum model");
         const int64_t R = ((int64_t)L->max_n + L->cluster - 1) / L->cluster;
         if (R > 480)
@@ -229,8 +236,14 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
                         (long long)R);
         if (L->cluster_edges < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster_edges < 0");
         const int64_t nacc = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
-        const int64_t b = ((R + 1) * 4 + 15) / 16 * 16 + (2 * R * nacc * 4 + 15) / 16 * 16 +
-                          (int64_t)L->cluster_edges * 8;
+        // edge runs: row pointers, double-buffered partials of all 512 threads, the edges
+        const int64_t b = E ? ((R + 1) * 4 + 15) / 16 * 16 + (2 * 512 * 2 * nacc * 4 + 15) / 16 * 16 +
+                                  (int64_t)L->cluster_edges * 8
+                            : ((R + 1) * 4 + 15) / 16 * 16 + (2 * R * nacc * 4 + 15) / 16 * 16 +
+                                  (int64_t)L->cluster_edges * 8;
+        if (E && L->cluster_edges <= 0)
+            return fail(TVBK_ERR_INVALID, "tvbk_sim_run: edge runs need the CTAs' edges in shared memory "
+                        "(cluster_edges > 0)");
         if (b > kMaxSmemPerBlock)
             return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: cluster CTA needs %lld bytes of shared memory",
                         (long long)b);
@@ -251,7 +264,7 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (threads > 1024 || b > kMaxSmemPerBlock)
             return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: a group of %d lanes x %d regions needs %lld threads and "
                         "%lld bytes of shared memory", L->lanes, L->max_n, (long long)threads, (long long)b);
-    } else if (L->edges_per_thread != 0) {
+    } else if (L->cluster <= 1 && L->edges_per_thread != 0) {
         const int E = L->edges_per_thread;
         if (E != 8 && E != 12 && E != 16 && E != 24)
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: edges_per_thread must be 0, 8, 12, 16 or 24");

@@ -44,6 +44,13 @@ constexpr int kClusterRowsPerPass = 4;
 
 __host__ __device__ inline int cluster_rows(int n, int C) { return (n + C - 1) / C; }
 
+// Shared memory of the edge-run variant: row pointers, then the double-buffered
+// partials ([2][threads][2][ng] floats), then the CTA's edges.
+__host__ __device__ inline size_t cluster_runs_head_rp(int R) { return ((size_t)(R + 1) * 4 + 15) / 16 * 16; }
+__host__ __device__ inline size_t cluster_runs_head(int R, int ng, int threads) {
+    return cluster_runs_head_rp(R) + ((size_t)2 * threads * 2 * ng * 4 + 15) / 16 * 16;
+}
+
 // Shared memory of one cluster CTA: row pointers, the double-buffered sums
 // and (when they fit) the CTA's edges.
 __host__ __device__ inline size_t cluster_smem_head(int R, int nacc) {
@@ -229,6 +236,236 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const t
     if (rank == 0 && tid == 0) Ip->step = s_end;
 }
 
+// Edge-run variant of the cluster kernel (launch.edges_per_thread = E > 0).
+// The CTA's edges, in CSR order and staged in shared memory, are cut into
+// runs of E consecutive edges, one run per gather thread.  With E at most the
+// smallest non-zero row degree of the CTA a run holds edges of at most two
+// rows -- its first row (partial a) and the next row with edges (partial b) --
+// so every thread issues E independent ring loads per step with no lane idle
+// beyond the last run, instead of a warp per row whose lanes run out of
+// edges unevenly.  The update thread of row r adds the partials of the runs
+// covering r in run order (a fixed order: the result does not depend on
+// timing).  Difference, w (x_j - x_i), is summed as sum_j w x_j - x_i sum_j w
+// with the row's weight sum W taken once in CSR order, so the gather needs no
+// x_i and, with PIPE, runs one step ahead like the other couplings.
+template <class M, int CF, int SCHEME, int E, bool PIPE, bool EXT = true>
+__global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(const tvbk_launch L) {
+    constexpr int NCV = M::NCV;
+    constexpr bool SIGMA = GatherTraits<CF, NCV>::SIGMA;
+    constexpr int NG = GatherTraits<CF, NCV>::NG;  // floats per gathered value and partial sums per run half
+    extern __shared__ __align__(16) unsigned char sm[];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x / C;
+    int32_t* status = L.status + blockIdx.x / C;
+    const int n = Ip->n;
+    const int R = cluster_rows(n, C);
+    const int r0 = min(n, rank * R), r1 = min(n, r0 + R), nr = r1 - r0;
+    const int RL = Ip->ring_len;
+    const int slot_floats = n * NG;
+    const int ring_floats = RL * slot_floats;
+    const int64_t s0 = Ip->step;
+    const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
+    if (s0 >= s_end) return;  // uniform over the cluster
+    const int nsteps = (int)(s_end - s0);
+    const int tid = threadIdx.x;
+    const int U = (nr + 31) >> 5;       // update warps
+    const int T0 = PIPE ? 32 * U : 0;   // first gather thread
+    const int Tg = blockDim.x - T0;     // gather threads
+
+    int* rp = reinterpret_cast<int*>(sm);
+    float* part = reinterpret_cast<float*>(sm + cluster_runs_head_rp(R));            // [2][blockDim][2][NG]
+    int2* esm = reinterpret_cast<int2*>(sm + cluster_runs_head(R, NG, blockDim.x));  // the CTA's edges
+    const int e_lo = Ip->row_ptr[r0], e_hi = Ip->row_ptr[r1];
+    const int ne = e_hi - e_lo;
+    // the runs must cover the CTA's edges and fit the launch's shared-memory allowance (planned on the host);
+    // a CTA whose edges do not fit flags the instance and takes part in every barrier without doing any work
+    // (no early return: the other CTAs of the cluster wait for it at the cluster barriers)
+    const bool fits = ne <= L.cluster_edges && ne <= Tg * E;
+    if (!fits && tid == 0) atomicOr(status, TVBK_STATUS_DEGREE);
+    const int2* eg = reinterpret_cast<const int2*>(Ip->edges) + e_lo;
+    for (int k = tid; k <= nr; k += blockDim.x) rp[k] = Ip->row_ptr[r0 + k] - e_lo;
+    if (fits)
+        for (int k = tid; k < ne; k += blockDim.x) esm[k] = __ldg(eg + k);
+
+    float cf[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cf[k] = Ip->cfun[k];
+    const bool upd = fits && tid < nr;
+    Node<M, SCHEME, EXT> node;
+    if (upd) {
+        node.init(L, Ip, r0 + tid, n, s0);
+        if (Ip->aff != nullptr || (!EXT && (Ip->stim != nullptr || Ip->proj != nullptr)))
+            atomicOr(status, TVBK_STATUS_UNSUPPORTED);
+    }
+    float* __restrict__ raw = Ip->ring;
+    float* __restrict__ ring = SIGMA ? Ip->pre_ring : raw;
+    if constexpr (SIGMA) {
+        sigma_ring(ring, raw, RL * n, rank * blockDim.x + tid, C * blockDim.x, cf);
+        cluster.sync();
+    } else {
+        __syncthreads();
+    }
+
+    // this thread's run: edges [eb, eb + cnt), the first kb of them in its first row
+    const int g = tid - T0;
+    const int eb = g * E;
+    const int cnt = (fits && g >= 0) ? max(0, min(E, ne - eb)) : 0;
+    int kb = cnt;
+    if (cnt > 0) {
+        int lo = 0, hi = nr - 1;  // the row of edge eb: the largest lr with rp[lr] <= eb
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (rp[mid] <= eb) lo = mid; else hi = mid - 1;
+        }
+        kb = min(rp[lo + 1] - eb, cnt);
+        if (kb < cnt) {  // the rest must lie in one row: the next one with edges
+            int r2 = lo + 1;
+            while (rp[r2 + 1] == rp[r2]) ++r2;
+            if (rp[r2 + 1] < eb + cnt) atomicOr(status, TVBK_STATUS_DEGREE);
+        }
+    }
+    // which partials make up row tid (update threads): half sf of run tf, then half a of runs tf+1 .. tl;
+    // for Difference also the row's weight sum
+    int tf = -1, sf = 0, tl = -1;
+    float wsum = 0.0f;
+    if (upd && rp[tid + 1] > rp[tid]) {
+        tf = rp[tid] / E;
+        sf = (rp[tid] == tf * E) ? 0 : 1;
+        tl = (rp[tid + 1] - 1) / E;
+        if constexpr (CF == CF_DIFFERENCE)
+            for (int e = rp[tid]; e < rp[tid + 1]; ++e) wsum += __int_as_float(esm[e].y);
+    }
+    __syncthreads();
+
+    const size_t half = (size_t)blockDim.x * 2 * NG;  // floats of one buffer of partials
+    auto gather = [&](int prev, int buf) {
+        const int base_off = prev * slot_floats;
+        float pa[NG], pb[NG];
+#pragma unroll
+        for (int q = 0; q < NG; ++q) pa[q] = pb[q] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            if (k < cnt) {
+                const int2 ed = esm[eb + k];
+                float v[NG];
+                load_cg<NG>(ring + gather_addr(base_off, ed.x, ring_floats), v);
+                const float w = __int_as_float(ed.y);
+                const float wa = k < kb ? w : 0.0f, wb = k < kb ? 0.0f : w;
+#pragma unroll
+                for (int q = 0; q < NG; ++q) {
+                    pa[q] = fmaf(wa, v[q], pa[q]);
+                    pb[q] = fmaf(wb, v[q], pb[q]);
+                }
+            }
+        }
+        float* out = part + buf * half + (size_t)g * 2 * NG;
+#pragma unroll
+        for (int q = 0; q < NG; ++q) {
+            out[q] = pa[q];
+            out[NG + q] = pb[q];
+        }
+    };
+    auto update = [&](int ks, int wslot, int buf) {
+        const float* in = part + buf * half;
+        float a[NG], c[NCV];
+#pragma unroll
+        for (int q = 0; q < NG; ++q) a[q] = 0.0f;
+        if (tf >= 0) {
+#pragma unroll
+            for (int q = 0; q < NG; ++q) a[q] = in[(size_t)tf * 2 * NG + sf * NG + q];
+            for (int u = tf + 1; u <= tl; ++u) {
+#pragma unroll
+                for (int q = 0; q < NG; ++q) a[q] += in[(size_t)u * 2 * NG + q];
+            }
+        }
+        if constexpr (CF == CF_DIFFERENCE) {
+            // sum_j w (x_j - x_i) = sum_j w x_j - x_i W, x_i the row's coupling variables at time s - 1
+#pragma unroll
+            for (int q = 0; q < NG; ++q) a[q] = fmaf(-node.x[M::cvar(q)], wsum, a[q]);
+        }
+        post<CF, NCV>(a, cf, c);
+        if (STOCH_BLOCK_START(ks)) node.noise_block(L, r0 + tid, s0 + 1 + ks);
+        node.advance(L, Ip, r0 + tid, n, s0, ks, c);
+        node.write_ring(raw + (size_t)wslot * n * NCV + (r0 + tid) * NCV);
+        if constexpr (SIGMA)
+            ring[wslot * slot_floats + r0 + tid] = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+    };
+
+    const int K = L.sync_every;
+    int since_sync = 0;
+    int wslot = (int)(s0 % RL);  // slot of the last written time
+    if constexpr (PIPE) {
+        if (g >= 0) gather(wslot, 0);
+        __syncthreads();
+    }
+    for (int ks = 0; ks < nsteps; ++ks) {
+        const int prev = wslot;
+        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
+        if constexpr (PIPE) {
+            if (tid < T0) {
+                if (upd) update(ks, wslot, ks & 1);
+            } else if (ks + 1 < nsteps) {
+                gather(wslot, (ks + 1) & 1);  // step s + 1: times <= s - d_min
+            }
+            __syncthreads();
+        } else {
+            gather(prev, 0);
+            __syncthreads();
+            if (upd) update(ks, wslot, 0);
+            __syncthreads();
+        }
+        if (++since_sync == K) {
+            since_sync = 0;
+            cluster.sync();
+        }
+    }
+    cluster.sync();
+    if (upd) node.finish(L, Ip, r0 + tid, n, status);
+    if (rank == 0 && tid == 0) Ip->step = s_end;
+}
+
+template <class M, int CF, int SCHEME, int E, bool PIPE, bool EXT>
+int launch_cluster_runs_t(const tvbk_launch& L, cudaStream_t st) {
+    auto kern = sim_kernel_cluster_runs<M, CF, SCHEME, E, PIPE, EXT>;
+    constexpr int NG = GatherTraits<CF, M::NCV>::NG;
+    const int C = L.cluster;
+    const int R = cluster_rows(L.max_n, C);
+    const size_t smem = cluster_runs_head(R, NG, kClusterThreads) + (size_t)L.cluster_edges * 8;
+    if (smem > 227 * 1024) return -1;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    if (C > 8) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return (int)e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(L.n_inst * C), 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, kern, L);
+    return (int)e;
+}
+
+template <class M, int CF, int SCHEME, bool PIPE, bool EXT>
+int launch_cluster_runs(const tvbk_launch& L, cudaStream_t st) {
+    switch (L.edges_per_thread) {
+        case 8: return launch_cluster_runs_t<M, CF, SCHEME, 8, PIPE, EXT>(L, st);
+        case 16: return launch_cluster_runs_t<M, CF, SCHEME, 16, PIPE, EXT>(L, st);
+        case 32: return launch_cluster_runs_t<M, CF, SCHEME, 32, PIPE, EXT>(L, st);
+        default: return -2;
+    }
+}
+
 template <class M, int CF, int SCHEME, int MAXE, bool PIPE, bool EXT>
 int launch_cluster_t(const tvbk_launch& L, cudaStream_t st) {
     auto kern = sim_kernel_cluster<M, CF, SCHEME, MAXE, PIPE, EXT>;
@@ -270,6 +507,16 @@ int launch_cluster_p(const tvbk_launch& L, cudaStream_t st) {
 
 template <class M, int CF, int SCHEME>
 int launch_cluster(const tvbk_launch& L, cudaStream_t st) {
+    if (L.edges_per_thread > 0) {  // edge runs
+        if (L.extras == 0) {
+            if (L.prefetch) return launch_cluster_runs<M, CF, SCHEME, true, false>(L, st);
+            return launch_cluster_runs<M, CF, SCHEME, false, false>(L, st);
+        }
+        if (L.prefetch) return launch_cluster_runs<M, CF, SCHEME, true, true>(L, st);
+        return launch_cluster_runs<M, CF, SCHEME, false, true>(L, st);
+    }
+    // the warp-per-row gather reads x_i of the step it sums: no prefetch with Difference
+    if (CF == CF_DIFFERENCE && L.prefetch) return -2;
     if (L.extras == 0) {
         if (L.prefetch) return launch_cluster_p<M, CF, SCHEME, true, false>(L, st);
         return launch_cluster_p<M, CF, SCHEME, false, false>(L, st);

@@ -314,6 +314,14 @@ class Batch:
         # mirrored guard slots past a shared-memory ring (prefetch 1; the split kernel has none)
         self.guard = _lib.RING_GUARD if (self.prefetch == 1 and self.ring_in_smem and V == 1) else 0
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
+        if self.cluster:
+            # edge runs for the cluster CTAs when they fit; with them Difference also prefetches
+            runs = self._choose_cluster_runs(dmin)
+            if runs:
+                self.edges_per_thread = runs
+                if dmin >= 1 and self.cfun_id == _lib.CFUN_IDS['Difference']:
+                    self.prefetch = 1
+                    self.sync_every = min(self.sync_every, dmin)
         self.slot_width, self._ring_len = self._choose_slots()
         self._plan()
         self.allocated = False
@@ -440,6 +448,46 @@ class Batch:
                 hi = min(n, lo + R)
                 emax = max(emax, int(rp[hi] - rp[lo]))
         return C, (emax if head + 8 * emax <= self.CLUSTER_SMEM else 0)
+
+    CLUSTER_THREADS = 512
+    CLUSTER_RUNS = (8, 16, 32)
+
+    def _choose_cluster_runs(self, dmin):
+        """Edge-run length of the cluster kernel, or 0 for a warp per row: the
+        smallest E of CLUSTER_RUNS whose runs cover every CTA's edges with the
+        CTA's gather threads (512, less one update warp per 32 rows when the
+        gather runs a step ahead) and that does not exceed the smallest
+        non-zero row degree of any CTA (a run then holds at most two rows).
+        Needs every CTA's edges in shared memory with the larger partials
+        buffer of the run kernel."""
+        if not self.cluster_edges:
+            return 0
+        C = self.cluster
+        R = -(-self.max_n // C)
+        nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
+        head = -(-(R + 1) * 4 // 16) * 16 + -(-2 * self.CLUSTER_THREADS * 2 * nacc * 4 // 16) * 16
+        if head + 8 * self.cluster_edges > self.CLUSTER_SMEM:
+            return 0
+        ahead = dmin >= 1 and self.model_id != _lib.MODEL_IDS['Sum']
+        need, cap = 1, 1 << 30
+        for s in self.specs:
+            rp = np.asarray(s.conn.row_ptr)
+            deg = np.diff(rp)
+            n = s.conn.n
+            for r in range(C):
+                lo, hi = min(n, r * R), min(n, r * R + R)
+                nr = hi - lo
+                if nr == 0:
+                    continue
+                tg = self.CLUSTER_THREADS - (32 * -(-nr // 32) if ahead else 0)
+                need = max(need, -(-int(rp[hi] - rp[lo]) // tg))
+                d = deg[lo:hi]
+                if (d > 0).any():
+                    cap = min(cap, int(d[d > 0].min()))
+        for E in self.CLUSTER_RUNS:
+            if need <= E <= cap:
+                return E
+        return 0
 
     EP_SLOTS = (8, 12, 16, 24)
 

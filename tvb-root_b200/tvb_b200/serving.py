@@ -137,7 +137,7 @@ class SimulationServer:
         # cluster, prefetch, sigmoid ring), so every occupant of a launch has the buffers that launch reads
         key = (sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, float(np.float32(sim.integrator.dt)),
                tuple(sim._voi_codes), sim.number_of_nodes, plan.ring_in_smem, plan.cluster, plan.prefetch,
-               plan.sigma)
+               plan.sigma, plan.edges_per_thread if plan.cluster else 0)
         req = _Request(rid, sim, spec, noise_kind, key, plan, time.perf_counter() if t_submit is None else t_submit)
         if req.footprint > self.budget:
             raise ValueError('request needs %d bytes, more than the budget of %d' % (req.footprint, self.budget))
@@ -213,6 +213,7 @@ class SimulationServer:
         L.lanes = 1
         L.cluster = p0.cluster
         L.cluster_edges = max(p.cluster_edges for p in plans)
+        L.edges_per_thread = p0.edges_per_thread if p0.cluster else 0   # edge runs (one value per group)
         L.extras = 0
         for p in plans:
             L.extras |= p.extras
