@@ -238,7 +238,7 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         const int64_t nacc = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
         // edge runs: row pointers, double-buffered partials of all 512 threads, the edges
         const int64_t b = E ? ((R + 1) * 4 + 15) / 16 * 16 + (2 * 512 * 2 * nacc * 4 + 15) / 16 * 16 +
-                                  (int64_t)L->cluster_edges * 8
+                                  ((int64_t)L->cluster_edges + E) * 8
                             : ((R + 1) * 4 + 15) / 16 * 16 + (2 * R * nacc * 4 + 15) / 16 * 16 +
                                   (int64_t)L->cluster_edges * 8;
         if (E && L->cluster_edges <= 0)

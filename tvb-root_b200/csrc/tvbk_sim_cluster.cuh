@@ -275,8 +275,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
     const int Tg = blockDim.x - T0;     // gather threads
 
     int* rp = reinterpret_cast<int*>(sm);
-    float* part = reinterpret_cast<float*>(sm + cluster_runs_head_rp(R));            // [2][blockDim][2][NG]
-    int2* esm = reinterpret_cast<int2*>(sm + cluster_runs_head(R, NG, blockDim.x));  // the CTA's edges
+    float* part = reinterpret_cast<float*>(sm + cluster_runs_head_rp(R));            // [2][2 NG][blockDim]
+    int2* esm = reinterpret_cast<int2*>(sm + cluster_runs_head(R, NG, blockDim.x));  // the CTA's edges, interleaved
     const int e_lo = Ip->row_ptr[r0], e_hi = Ip->row_ptr[r1];
     const int ne = e_hi - e_lo;
     // the runs must cover the CTA's edges and fit the launch's shared-memory allowance (planned on the host);
@@ -286,8 +286,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
     if (!fits && tid == 0) atomicOr(status, TVBK_STATUS_DEGREE);
     const int2* eg = reinterpret_cast<const int2*>(Ip->edges) + e_lo;
     for (int k = tid; k <= nr; k += blockDim.x) rp[k] = Ip->row_ptr[r0 + k] - e_lo;
+    // edge e (CSR order) is edge k = e % E of run g = e / E, kept at slot k * nrun + g: at every k the threads
+    // of a warp read consecutive 8-byte words (one wavefront), where runs side by side would all read one bank
+    const int nrun = (ne + E - 1) / E;
+    auto eslot = [&](int e) { return (e % E) * nrun + e / E; };
     if (fits)
-        for (int k = tid; k < ne; k += blockDim.x) esm[k] = __ldg(eg + k);
+        for (int e = tid; e < ne; e += blockDim.x) esm[eslot(e)] = __ldg(eg + e);
 
     float cf[6];
 #pragma unroll
@@ -335,11 +339,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
         sf = (rp[tid] == tf * E) ? 0 : 1;
         tl = (rp[tid + 1] - 1) / E;
         if constexpr (CF == CF_DIFFERENCE)
-            for (int e = rp[tid]; e < rp[tid + 1]; ++e) wsum += __int_as_float(esm[e].y);
+            for (int e = rp[tid]; e < rp[tid + 1]; ++e) wsum += __int_as_float(esm[eslot(e)].y);
     }
     __syncthreads();
 
-    const size_t half = (size_t)blockDim.x * 2 * NG;  // floats of one buffer of partials
+    const size_t half = (size_t)blockDim.x * 2 * NG;  // floats of one buffer of partials: [2 NG][blockDim]
+    const int TB = blockDim.x;
     auto gather = [&](int prev, int buf) {
         const int base_off = prev * slot_floats;
         float pa[NG], pb[NG];
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 #pragma unroll
         for (int k = 0; k < E; ++k) {
             if (k < cnt) {
-                const int2 ed = esm[eb + k];
+                const int2 ed = esm[k * nrun + g];
                 float v[NG];
                 load_cg<NG>(ring + gather_addr(base_off, ed.x, ring_floats), v);
                 const float w = __int_as_float(ed.y);
@@ -360,11 +365,11 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
                 }
             }
         }
-        float* out = part + buf * half + (size_t)g * 2 * NG;
+        float* out = part + buf * half + g;
 #pragma unroll
         for (int q = 0; q < NG; ++q) {
-            out[q] = pa[q];
-            out[NG + q] = pb[q];
+            out[q * TB] = pa[q];
+            out[(NG + q) * TB] = pb[q];
         }
     };
     auto update = [&](int ks, int wslot, int buf) {
@@ -374,10 +379,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
         for (int q = 0; q < NG; ++q) a[q] = 0.0f;
         if (tf >= 0) {
 #pragma unroll
-            for (int q = 0; q < NG; ++q) a[q] = in[(size_t)tf * 2 * NG + sf * NG + q];
+            for (int q = 0; q < NG; ++q) a[q] = in[(size_t)(sf * NG + q) * TB + tf];
             for (int u = tf + 1; u <= tl; ++u) {
 #pragma unroll
-                for (int q = 0; q < NG; ++q) a[q] += in[(size_t)u * 2 * NG + q];
+                for (int q = 0; q < NG; ++q) a[q] += in[(size_t)q * TB + u];
             }
         }
         if constexpr (CF == CF_DIFFERENCE) {
@@ -432,7 +437,8 @@ int launch_cluster_runs_t(const tvbk_launch& L, cudaStream_t st) {
     constexpr int NG = GatherTraits<CF, M::NCV>::NG;
     const int C = L.cluster;
     const int R = cluster_rows(L.max_n, C);
-    const size_t smem = cluster_runs_head(R, NG, kClusterThreads) + (size_t)L.cluster_edges * 8;
+    // interleaved runs take up to cluster_edges + E - 1 edge slots
+    const size_t smem = cluster_runs_head(R, NG, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
     if (smem > 227 * 1024) return -1;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;

@@ -466,7 +466,7 @@ class Batch:
         R = -(-self.max_n // C)
         nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
         head = -(-(R + 1) * 4 // 16) * 16 + -(-2 * self.CLUSTER_THREADS * 2 * nacc * 4 // 16) * 16
-        if head + 8 * self.cluster_edges > self.CLUSTER_SMEM:
+        if head + 8 * (self.cluster_edges + max(self.CLUSTER_RUNS)) > self.CLUSTER_SMEM:
             return 0
         ahead = dmin >= 1 and self.model_id != _lib.MODEL_IDS['Sum']
         need, cap = 1, 1 << 30
