@@ -215,9 +215,10 @@ typedef struct tvbk_launch {
                                   * lets the row kernel with rings in shared memory use a build without any of
                                   * them (an instance that has one then gets TVBK_STATUS_UNSUPPORTED) */
     const int32_t* inst_order;   /* device [n_inst] or NULL: CTA b advances insts[inst_order[b]] and ORs its status
-                                  * bits into status[inst_order[b]] (row kernel only: lanes 1, no cluster, no edge
-                                  * split, prefetch 0 or 1).  Lets one launch take any subset of a batch, e.g. a
-                                  * window of exactly one wave of resident CTAs */
+                                  * bits into status[inst_order[b]] (row kernel: lanes 1, no edge split, prefetch 0
+                                  * or 1; with cluster > 1, cluster b advances insts[inst_order[b]]).  Lets one
+                                  * launch take any subset of a batch, e.g. a window of exactly one wave of resident
+                                  * CTAs, or order it, e.g. the longest instances first */
     int32_t* occupancy;          /* host pointer or NULL: when set, tvbk_sim_run launches nothing and stores there
                                   * the CTAs per SM of the row kernel variant it would launch (same restrictions) */
     int64_t max_steps;           /* steps per launch (a chunk); instances stop at step_end */

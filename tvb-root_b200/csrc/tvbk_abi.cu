@@ -200,10 +200,12 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: prefetch 2 (separate gather warps) needs rings in shared memory, "
                     "the row gather (lanes 1, no edge split, no cluster), Linear or SigmoidalJansenRit coupling and "
                     "row degrees <= 64");
-    if ((L->inst_order || L->occupancy) &&
-        (L->lanes > 1 || L->cluster > 1 || L->edges_per_thread != 0 || L->prefetch == 2))
-        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: inst_order and occupancy apply to the row kernel (lanes 1, no "
+    if (L->occupancy && (L->lanes > 1 || L->cluster > 1 || L->edges_per_thread != 0 || L->prefetch == 2))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: occupancy applies to the row kernel (lanes 1, no "
                     "cluster, edges_per_thread 0, prefetch 0 or 1)");
+    if (L->inst_order && (L->lanes > 1 || (L->cluster <= 1 && L->edges_per_thread != 0) || L->prefetch == 2))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: inst_order applies to the row kernel (lanes 1, "
+                    "edges_per_thread 0, prefetch 0 or 1) and to the cluster kernel");
     if (L->max_steps < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: max_steps < 0");
     if (!(L->dt > 0.0f)) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: dt must be > 0");
     const bool stoch = L->scheme == TVBK_SCHEME_EULER_STOCH || L->scheme == TVBK_SCHEME_HEUN_STOCH;

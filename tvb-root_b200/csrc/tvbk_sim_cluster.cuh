@@ -98,8 +98,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster(const t
     cgx::cluster_group cluster = cgx::this_cluster();
     const int C = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
-    tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x / C;
-    int32_t* status = L.status + blockIdx.x / C;
+    // this cluster's instance: the launch may order the instances through inst_order (longest first)
+    const int inst = L.inst_order != nullptr ? L.inst_order[blockIdx.x / C] : (int)(blockIdx.x / C);
+    tvbk_inst* __restrict__ Ip = L.insts + inst;
+    int32_t* status = L.status + inst;
     const int n = Ip->n;
     const int R = cluster_rows(n, C);
     const int r0 = min(n, rank * R), r1 = min(n, r0 + R), nr = r1 - r0;
@@ -257,8 +259,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
     cgx::cluster_group cluster = cgx::this_cluster();
     const int C = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
-    tvbk_inst* __restrict__ Ip = L.insts + blockIdx.x / C;
-    int32_t* status = L.status + blockIdx.x / C;
+    // this cluster's instance: the launch may order the instances through inst_order (longest first)
+    const int inst = L.inst_order != nullptr ? L.inst_order[blockIdx.x / C] : (int)(blockIdx.x / C);
+    tvbk_inst* __restrict__ Ip = L.insts + inst;
+    int32_t* status = L.status + inst;
     const int n = Ip->n;
     const int R = cluster_rows(n, C);
     const int r0 = min(n, rank * R), r1 = min(n, r0 + R), nr = r1 - r0;

@@ -750,6 +750,11 @@ class Batch:
         self._upload_rings(ring_up)
         self.steps_done = 0
         self.max_total = max(s.n_steps for s in specs)
+        self._longest_first = None
+        lengths = np.array([s.n_steps for s in specs])
+        if self.cluster and len(set(lengths.tolist())) > 1:
+            order = np.argsort(-lengths, kind='stable').astype(np.int32)
+            self._longest_first = torch.as_tensor(order, device=dev)
 
     def _upload_rings(self, ring_up):
         """Host-to-device copy of each distinct initial ring, then device copies
@@ -831,6 +836,10 @@ class Batch:
         L.prefetch = self.prefetch
         L.max_steps = int(max_steps)
         L.dt = self.dt
+        if self.cluster and getattr(self, "_longest_first", None) is not None:
+            # clusters dispatch in launch order: the longest instances start first, so that the batch's
+            # last steps do not run one long instance alone
+            L.inst_order = self._longest_first.data_ptr()
         return L
 
     def occupancy(self):
