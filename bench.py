@@ -373,7 +373,7 @@ def run_serving(args, rank, local):
 EPI_N, EPI_DT = 998, 0.05
 
 
-def large_network_sweep(length_scale=1.0, check_ms=None, gather='auto', cluster='auto'):
+def large_network_sweep(length_scale=1.0, check_ms=None, gather='auto', cluster='auto', n_inst=16):
     """Epileptor, 998 regions (10 % density, tract lengths 5-300 mm, speed
     3 mm/ms), Difference coupling, HeunDeterministic dt 0.05 ms, 16 instances
     with x0 uniform in [-2.4, -1.6] per region and uneven lengths of 2-20 s
@@ -383,8 +383,8 @@ def large_network_sweep(length_scale=1.0, check_ms=None, gather='auto', cluster=
     from tvb_b200.connectivity import Connectivity
     from tvb_b200.sweep import ParameterSweep
     w, L = synthetic.connectome(EPI_N, 0.10, 5.0, 300.0, seed=4)
-    x0 = np.random.default_rng(14).uniform(-2.4, -1.6, (16, EPI_N))
-    lengths = np.linspace(2000.0, 20000.0, 16) * length_scale
+    x0 = np.random.default_rng(14).uniform(-2.4, -1.6, (16, EPI_N))[:n_inst]
+    lengths = (np.linspace(2000.0, 20000.0, 16) * length_scale)[:n_inst]
     np.random.seed(15)
     sweep = {'model.x0': x0} if check_ms else {'model.x0': x0, 'simulation_length': lengths}
     sw = ParameterSweep(model=models.Epileptor(), connectivity=Connectivity(w, L, speed=3.0),
@@ -444,11 +444,12 @@ def large_network_error(check_ms, cores):
             'nonfinite_instances': int((res['status'] != 0).sum()), 'oracle_wall_s': wall}
 
 
-def large_network_leg(steps, warmup, local, length_scale=1.0, gather='auto', cluster='auto'):
-    """Region-steps/s of the 16-instance large-network batch on the device."""
+def large_network_leg(steps, warmup, local, length_scale=1.0, gather='auto', cluster='auto', n_inst=16):
+    """Region-steps/s of the 16-instance large-network batch on the device
+    (n_inst < 16: its first n_inst instances)."""
     import torch
     torch.cuda.set_device(local)
-    sw, x0, lengths = large_network_sweep(length_scale, gather=gather, cluster=cluster)
+    sw, x0, lengths = large_network_sweep(length_scale, gather=gather, cluster=cluster, n_inst=n_inst)
     b = sw.build()
     b.snapshot()
     st = torch.cuda.current_stream()
@@ -465,17 +466,18 @@ def large_network_leg(steps, warmup, local, length_scale=1.0, gather='auto', clu
     steps_total = int(sw.n_steps_each.sum())
     t = float(np.mean(ms)) / 1e3
     return {'value': float(steps_total * EPI_N / t), 'unit': UNIT, 'ms_per_step': 1e3 * t, 'steps': steps,
-            'warmup': warmup, 'instances': 16, 'regions': EPI_N, 'nnz': int(sw._sim._conn.nnz), 'dt_ms': EPI_DT,
+            'warmup': warmup, 'instances': n_inst, 'regions': EPI_N, 'edge_runs': b.edges_per_thread, 'nnz': int(sw._sim._conn.nnz), 'dt_ms': EPI_DT,
             'lengths_ms': lengths.tolist(), 'cluster_ctas_per_instance': b.cluster, 'sync_every': b.sync_every,
             'nonfinite_instances': int((b.status() != 0).sum()), 'gpu_launches': steps * b.last_launches}
 
 
 def run_large_network(args, rank, local):
-    leg = large_network_leg(args.steps, args.warmup, local, args.length / 60000.0, args.gather, args.cluster)
+    leg = large_network_leg(args.steps, args.warmup, local, args.length / 60000.0, args.gather, args.cluster,
+                            args.ln_instances)
     line = {'metric': 'region-steps/sec, large-network batch', 'value': leg['value'], 'unit': UNIT,
             'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': leg['ms_per_step'],
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': 'epileptor_998r_16i_uneven_2-20s', 'instances': 16, 'regions': EPI_N,
+            'config': {'workload': 'epileptor_998r_16i_uneven_2-20s', 'instances': leg['instances'], 'regions': EPI_N,
                        'nnz': leg['nnz'], 'dt_ms': EPI_DT, 'lengths_ms': leg['lengths_ms'],
                        'cluster_ctas_per_instance': leg['cluster_ctas_per_instance'],
                        'sync_every': leg['sync_every']},
@@ -486,9 +488,9 @@ def run_large_network(args, rank, local):
 
 
 # DRAM bytes per instance-step of the simulation kernel on this workload, from the ncu capture
-# of 296 instances x 40 000 steps (dram__bytes_read.sum + dram__bytes_write.sum = 1.797 GB);
+# of 296 instances x 40 000 steps (dram__bytes_read.sum + dram__bytes_write.sum = 1.786 GB);
 # a launch's traffic scales with its instance-steps.
-NCU_DRAM_BYTES_PER_INSTANCE_STEP = 1.771e9 / (296 * 40000)
+NCU_DRAM_BYTES_PER_INSTANCE_STEP = 1.786e9 / (296 * 40000)
 
 
 # --------------------------------------------------------------------- main
@@ -552,6 +554,8 @@ def main():
                     help='steps of the Philox-path parity check against the oracle (0 skips it)')
     ap.add_argument('--check-ms', type=float, default=60.0,
                     help='large network: ms of the per-instance error check against the oracle (0 skips it)')
+    ap.add_argument('--ln-instances', type=int, default=16, choices=range(1, 17), metavar='1..16',
+                    help='large network: run the first k of the 16 instances')
     ap.add_argument('--no-legs', action='store_true',
                     help='sweep only: no serving and large-network legs in the line')
     args = ap.parse_args()
