@@ -402,8 +402,8 @@ def test_kernel_variants_agree(cfun):
     (separate gather and update warps, same summation order), the edge-parallel
     kernel (balanced edge split, row partials), the instance-lane kernels (2
     and 4 interleaved instances) and the cluster kernel (4 and 16 CTAs per
-    instance, warp-per-row gather) compute the same trajectories up to
-    float32 summation order."""
+    instance, edge runs; Difference then sums w x_j - x_i W and prefetches)
+    compute the same trajectories up to float32 summation order."""
     import bench
     from tvb_b200 import coupling, integrators, models, monitors, noise, synthetic
     from tvb_b200.connectivity import Connectivity
@@ -450,6 +450,8 @@ def test_kernel_variants_agree(cfun):
         if gather == 'edge':
             assert sw.batch.edges_per_thread > 0
         assert sw.batch.cluster == cluster
+        if cluster:
+            assert sw.batch.edges_per_thread in (8, 16, 32) and sw.batch.prefetch == 1, (cluster, sw.batch.edges_per_thread)
         out[key] = res
     base = out[('row', 1, True, 0)]
     for key, res in out.items():
