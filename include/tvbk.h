@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define TVBK_ABI_VERSION 1
+#define TVBK_ABI_VERSION 2
 
 /* status codes */
 #define TVBK_OK 0
@@ -210,6 +210,14 @@ typedef struct tvbk_launch {
                                   * place (lanes 1, row gather, rings not in shared memory) */
     int32_t cluster_edges;       /* cluster kernel: edges of one CTA's rows that it stages in shared memory; a CTA
                                   * with more edges reads them from global memory (0: always global) */
+    int32_t ring_layout;         /* 0: rings [ring_len][n][ncvar] (time-major).  1: region-major rings for the
+                                  * cluster kernel's blocked edge runs (cluster > 1, edges_per_thread > 0,
+                                  * prefetch 1, Linear or Difference, ncvar 1 or 2, sync_every a multiple of 4
+                                  * with 4 <= sync_every <= the smallest delay - 3): region r's times sit in
+                                  * [r][TVBK_RING_REGION_STRIDE(ring_len, ncvar)][ncvar], time t in slot
+                                  * t % ring_len, and the slots past ring_len mirror slots 0, 1, ... (every write
+                                  * of a mirrored slot also writes its mirror).  Four steps' couplings are gathered
+                                  * together, each edge reading its four consecutive times with 16-byte loads */
     int32_t extras;              /* bit 0: some instance has a region stimulus; bit 1: some instance has an
                                   * AfferentCoupling monitor; bit 2: some instance has a projection stream.  0
                                   * lets the row kernel with rings in shared memory use a build without any of
@@ -255,6 +263,15 @@ int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weig
  * they mirror slots 0..TVBK_RING_GUARD-1, so that the gathers of four steps
  * in a row take one ring address per edge (address + r slots, r <= 3). */
 #define TVBK_RING_GUARD 3
+
+/* Region-major rings (launch.ring_layout = 1): slots per region -- the
+ * ring_len slots, then a guard of 5 (ncvar 2) or 7 (ncvar 1) slots mirroring
+ * slots 0, 1, ... (a four-step read loads a 48- or 32-byte window that may
+ * start just below ring_len), rounded up so that every region starts on a
+ * 16-byte boundary. */
+#define TVBK_RING_REGION_GUARD(ncvar) ((ncvar) == 1 ? 7 : 5)
+#define TVBK_RING_REGION_STRIDE(ring_len, ncvar) \
+    ((((ring_len) + TVBK_RING_REGION_GUARD(ncvar)) + (4 / (ncvar)) - 1) / (4 / (ncvar)) * (4 / (ncvar)))
 
 /* Smallest ring length (slots) usable with barrier interval sync_every. */
 int32_t tvbk_ring_len(int32_t horizon, int32_t sync_every);

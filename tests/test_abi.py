@@ -35,7 +35,7 @@ def test_every_declared_function_is_exported_and_bound():
 
 def test_struct_sizes_and_version():
     lib = _lib.load()
-    assert lib.tvbk_abi_version() == 1
+    assert lib.tvbk_abi_version() == 2
     assert lib.tvbk_sizeof(0) == ctypes.sizeof(_lib.Inst)
     assert lib.tvbk_sizeof(1) == ctypes.sizeof(_lib.Launch)
     assert lib.tvbk_sizeof(2) == 8

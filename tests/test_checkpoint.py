@@ -74,3 +74,36 @@ def test_resume_matches_uninterrupted_run(which):
         np.testing.assert_array_equal(np.concatenate([t for t in (ta, tb) if t.size]), tr)
         np.testing.assert_array_equal(np.concatenate([y for y in (ya, yb) if y.size]), yr)
     np.testing.assert_array_equal(resumed.history_buffer, whole.history_buffer)
+
+
+@pytest.mark.gpu
+def test_region_major_rings_resume_exactly():
+    """A large Epileptor network (998 regions) runs on the cluster kernel's blocked edge runs with region-major
+    rings; two run() calls -- the second re-uploads the history exported after the first -- give the bits of
+    one uninterrupted run, and the exported history has the reference's time-major layout."""
+    from tvb_b200 import synthetic
+
+    def make(length):
+        w, L = synthetic.connectome(998, 0.10, 5.0, 300.0, seed=4)
+        x0 = np.random.default_rng(14).uniform(-2.4, -1.6, 998)
+        np.random.seed(15)
+        return Simulator(model=models.Epileptor(x0=x0, Ks=np.array([-0.2]), Kf=np.array([0.05])),
+                         connectivity=Connectivity(w, L, speed=3.0), coupling=coupling.Difference(),
+                         integrator=integrators.HeunDeterministic(dt=0.05),
+                         monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=length).configure()
+    whole = make(20.0)
+    h0 = whole.history_buffer.copy()
+    spec, kind = whole.instance_spec(400)
+    from tvb_b200.engine import Batch
+    plan = Batch(whole._model_id, whole._cfun_id, whole._scheme_id, kind, 0.05, whole._voi_codes, [spec],
+                 allocate=False)
+    assert plan.cluster >= 2 and plan.ring_layout == 1 and plan.sync_every % 4 == 0
+    (t, y), = whole.run()
+    parts = make(20.0)
+    np.testing.assert_array_equal(parts.history_buffer, h0)
+    (t1, y1), = parts.run(n_steps=147)   # the first call ends inside a block of four steps
+    assert parts.history_buffer.shape == h0.shape
+    (t2, y2), = parts.run(n_steps=253)
+    np.testing.assert_array_equal(np.concatenate([t1, t2]), t)
+    np.testing.assert_array_equal(np.concatenate([y1, y2]), y)
+    np.testing.assert_array_equal(parts.current_state, whole.current_state)

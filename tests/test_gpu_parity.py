@@ -63,7 +63,7 @@ def test_gather_bit_exact(case, model, ncvar):
     for step0 in (0, 1, 17, H - 1, H, 3 * H + 5, 123457):
         spec = InstanceSpec(conn, buf, np.zeros((nsv, n), np.float32), np.zeros((nparam, n), np.float32), [0.0],
                             1, step0=step0)
-        batch = Batch(mid, 0, 2, 0, float(fx['dt']), [0], [spec], sync_every=7)
+        batch = Batch(mid, 0, 2, 0, float(fx['dt']), [0], [spec], sync_every=7, region_rings=False)
         got = batch.gather_delayed(0, step0 + 1)
         t_idx = (step0 + 1 - 1 - lay['d'] + H) % H
         # the reference buffer holds time t in slot t % H; re-slot the same content for step0

@@ -218,6 +218,8 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
                                            L->cluster > 1))
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: Sigmoidal, HyperbolicTangent and Kuramoto run on the row kernel "
                     "one step at a time (prefetch 0, lanes 1, edges_per_thread 0, cluster 0)");
+    if (L->ring_layout < 0 || L->ring_layout > 1 || (L->ring_layout == 1 && L->cluster <= 1))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: ring_layout 1 (region-major) applies to clusters only");
     if (L->cluster < 0 || L->cluster > 16)
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster %d out of 0..16", L->cluster);
     if (L->cluster > 1) {
@@ -228,6 +230,13 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (E != 0 && E != 8 && E != 16 && E != 32)
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster's edge runs have 8, 16 or 32 edges (or 0: a warp "
                         "per row)");
+        if (L->ring_layout == 1) {
+            if (E == 0 || L->prefetch != 1 || d.ncvar > 2 ||
+                (L->cfun != TVBK_CFUN_LINEAR && L->cfun != TVBK_CFUN_DIFFERENCE) || L->sync_every < 4 ||
+                L->sync_every % 4 != 0 || L->max_n > 1024)
+                return fail(TVBK_ERR_INVALID, "tvbk_sim_run: region-major rings need edge runs, prefetch 1, Linear or "
+                            "Difference coupling, ncvar <= 2, sync_every a multiple of 4 and at most 1024 regions");
+        }
         if (E == 0 && L->prefetch && L->cfun == TVBK_CFUN_DIFFERENCE)
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster with a warp per row cannot prefetch Difference "
                         "coupling (use edge runs)");
@@ -239,7 +248,8 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (L->cluster_edges < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster_edges < 0");
         const int64_t nacc = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
         // edge runs: row pointers, double-buffered partials of all 512 threads, the edges
-        const int64_t b = E ? ((R + 1) * 4 + 15) / 16 * 16 + (2 * 512 * 2 * nacc * 4 + 15) / 16 * 16 +
+        const int64_t nbuf = L->ring_layout == 1 ? 4 : 1;  // blocked runs keep the partials of four steps
+        const int64_t b = E ? ((R + 1) * 4 + 15) / 16 * 16 + (2 * nbuf * 512 * 2 * nacc * 4 + 15) / 16 * 16 +
                                   ((int64_t)L->cluster_edges + E) * 8
                             : ((R + 1) * 4 + 15) / 16 * 16 + (2 * R * nacc * 4 + 15) / 16 * 16 +
                                   (int64_t)L->cluster_edges * 8;

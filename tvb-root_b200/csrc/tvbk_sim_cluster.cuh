@@ -50,6 +50,10 @@ __host__ __device__ inline size_t cluster_runs_head_rp(int R) { return ((size_t)
 __host__ __device__ inline size_t cluster_runs_head(int R, int ng, int threads) {
     return cluster_runs_head_rp(R) + ((size_t)2 * threads * 2 * ng * 4 + 15) / 16 * 16;
 }
+// the blocked variant keeps the partials of four steps: [2][4][2][ng][threads] floats
+__host__ __device__ inline size_t cluster_blocks_head(int R, int ng, int threads) {
+    return cluster_runs_head_rp(R) + ((size_t)2 * 4 * threads * 2 * ng * 4 + 15) / 16 * 16;
+}
 
 // Shared memory of one cluster CTA: row pointers, the double-buffered sums
 // and (when they fit) the CTA's edges.
@@ -435,6 +439,271 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
     if (rank == 0 && tid == 0) Ip->step = s_end;
 }
 
+// Blocked edge runs on region-major rings (launch.ring_layout = 1).  The
+// runs are those of sim_kernel_cluster_runs, but the gather threads take four
+// steps at a time: for the next block of four steps an edge needs its
+// source's values at four consecutive times, which sit side by side in the
+// region-major ring -- one window of three (two for one coupling variable)
+// 16-byte L2 loads instead of four scattered 8-byte loads, each of which
+// costs a 32-byte sector.  The window starts on a 16-byte boundary at or
+// below the first time's slot and may run past ring_len into the region's
+// guard slots, which mirror slots 0, 1, ....  The update warps advance the
+// four steps of the current block from the partials gathered during the
+// previous block, so there is one CTA barrier per four steps.  The gather
+// of block b + 1 reads times up to 7 - d_min past the last time written
+// before block b, so it needs d_min >= 7 and a cluster barrier interval
+// K <= d_min - 3, a multiple of 4 (the windows start on block boundaries).
+template <class M, int CF, int SCHEME, int E, bool EXT = true>
+__global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(const tvbk_launch L) {
+    static_assert(CF == CF_LINEAR || CF == CF_DIFFERENCE, "blocked runs: Linear or Difference coupling");
+    constexpr int NCV = M::NCV;
+    constexpr int NG = NCV;
+    constexpr int SPC = 4 / NG;              // slots per 16-byte chunk
+    constexpr int NCH = NG == 2 ? 3 : 2;     // 16-byte chunks per four-step window
+    extern __shared__ __align__(16) unsigned char sm[];
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int inst = L.inst_order != nullptr ? L.inst_order[blockIdx.x / C] : (int)(blockIdx.x / C);
+    tvbk_inst* __restrict__ Ip = L.insts + inst;
+    int32_t* status = L.status + inst;
+    const int n = Ip->n;
+    const int R = cluster_rows(n, C);
+    const int r0 = min(n, rank * R), r1 = min(n, r0 + R), nr = r1 - r0;
+    const int RL = Ip->ring_len;
+    const int RS = TVBK_RING_REGION_STRIDE(RL, NG);  // slots per region
+    constexpr int GUARD = TVBK_RING_REGION_GUARD(NG);
+    const int64_t s0 = Ip->step;
+    const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
+    if (s0 >= s_end) return;  // uniform over the cluster
+    const int nsteps = (int)(s_end - s0);
+    const int tid = threadIdx.x;
+    const int TB = blockDim.x;
+    const int U = (nr + 31) >> 5;       // update warps
+    const int T0 = 32 * U;              // first gather thread
+    const int Tg = TB - T0;             // gather threads
+
+    int* rp = reinterpret_cast<int*>(sm);
+    float* part = reinterpret_cast<float*>(sm + cluster_runs_head_rp(R));            // [2][4][2][NG][TB]
+    int2* esm = reinterpret_cast<int2*>(sm + cluster_blocks_head(R, NG, TB));       // the CTA's edges, interleaved
+    const int e_lo = Ip->row_ptr[r0], e_hi = Ip->row_ptr[r1];
+    const int ne = e_hi - e_lo;
+    // as in sim_kernel_cluster_runs: a CTA whose edges do not fit flags the instance and only takes part in
+    // the barriers
+    const bool fits = ne <= L.cluster_edges && ne <= Tg * E;
+    if (!fits && tid == 0) atomicOr(status, TVBK_STATUS_DEGREE);
+    const int2* eg = reinterpret_cast<const int2*>(Ip->edges) + e_lo;
+    for (int k = tid; k <= nr; k += TB) rp[k] = Ip->row_ptr[r0 + k] - e_lo;
+    const int nrun = (ne + E - 1) / E;
+    auto eslot = [&](int e) { return (e % E) * nrun + e / E; };
+    // edge records {d * 1024 + col, weight}: the packed gather edge holds (d n - col) ncvar
+    if (fits)
+        for (int e = tid; e < ne; e += TB) {
+            int2 r = __ldg(eg + e);
+            const int x = r.x / NCV;
+            const int d = (x + n - 1) / n;
+            r.x = d * 1024 + (d * n - x);
+            esm[eslot(e)] = r;
+        }
+
+    float cf[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cf[k] = Ip->cfun[k];
+    const bool upd = fits && tid < nr;
+    Node<M, SCHEME, EXT> node;
+    if (upd) {
+        node.init(L, Ip, r0 + tid, n, s0);
+        if (Ip->aff != nullptr || (!EXT && (Ip->stim != nullptr || Ip->proj != nullptr)))
+            atomicOr(status, TVBK_STATUS_UNSUPPORTED);
+    }
+    float* __restrict__ ring = Ip->ring;
+    __syncthreads();
+
+    // this thread's run and the partials of row tid, as in sim_kernel_cluster_runs
+    const int g = tid - T0;
+    const int eb = g * E;
+    const int cnt = (fits && g >= 0) ? max(0, min(E, ne - eb)) : 0;
+    int kb = cnt;
+    if (cnt > 0) {
+        int lo = 0, hi = nr - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (rp[mid] <= eb) lo = mid; else hi = mid - 1;
+        }
+        kb = min(rp[lo + 1] - eb, cnt);
+        if (kb < cnt) {
+            int r2 = lo + 1;
+            while (rp[r2 + 1] == rp[r2]) ++r2;
+            if (rp[r2 + 1] < eb + cnt) atomicOr(status, TVBK_STATUS_DEGREE);
+        }
+    }
+    int tf = -1, sf = 0, tl = -1;
+    float wsum = 0.0f;
+    if (upd && rp[tid + 1] > rp[tid]) {
+        tf = rp[tid] / E;
+        sf = (rp[tid] == tf * E) ? 0 : 1;
+        tl = (rp[tid + 1] - 1) / E;
+        if constexpr (CF == CF_DIFFERENCE)
+            for (int e = rp[tid]; e < rp[tid + 1]; ++e) wsum += __int_as_float(esm[eslot(e)].y);
+    }
+
+    // partial (buffer pb, step r of the block, half h, variable q) of run u
+    auto pidx = [&](int pb, int r, int h, int q, int u) { return ((((pb * 4 + r) * 2 + h) * NG + q) * TB) + u; };
+    // couplings of the four steps after the time in slot st0: step r reads times (that time) + r - d
+    auto gather4 = [&](int st0, int pb) {
+        float pa[4][NG], pbs[4][NG];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < NG; ++q) pa[r][q] = pbs[r][q] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < E; ++k) {
+            if (k < cnt) {
+                const int2 ed = esm[k * nrun + g];
+                const int d = ed.x >> 10, col = ed.x & 1023;
+                int sl = st0 - d;
+                sl += sl < 0 ? RL : 0;
+                const int a = sl & ~(SPC - 1), o = sl - a;
+                const float4* src = reinterpret_cast<const float4*>(ring + ((size_t)col * RS + a) * NG);
+                float win[NCH * 4];
+#pragma unroll
+                for (int c = 0; c < NCH; ++c) {
+                    const float4 t = __ldcg(src + c);
+                    win[4 * c] = t.x;
+                    win[4 * c + 1] = t.y;
+                    win[4 * c + 2] = t.z;
+                    win[4 * c + 3] = t.w;
+                }
+                const float w = __int_as_float(ed.y);
+                const float wa = k < kb ? w : 0.0f, wb = k < kb ? 0.0f : w;
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int q = 0; q < NG; ++q) {
+                        float v;
+                        if constexpr (NG == 2) {
+                            v = o ? win[(r + 1) * 2 + q] : win[r * 2 + q];
+                        } else {
+                            v = o == 0 ? win[r] : (o == 1 ? win[r + 1] : (o == 2 ? win[r + 2] : win[r + 3]));
+                        }
+                        pa[r][q] = fmaf(wa, v, pa[r][q]);
+                        pbs[r][q] = fmaf(wb, v, pbs[r][q]);
+                    }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < NG; ++q) {
+                part[pidx(pb, r, 0, q, g)] = pa[r][q];
+                part[pidx(pb, r, 1, q, g)] = pbs[r][q];
+            }
+    };
+    auto update = [&](int ks, int wslot, int pb, int r) {
+        float a[NG], c[NCV];
+#pragma unroll
+        for (int q = 0; q < NG; ++q) a[q] = 0.0f;
+        if (tf >= 0) {
+#pragma unroll
+            for (int q = 0; q < NG; ++q) a[q] = part[pidx(pb, r, sf, q, tf)];
+            for (int u = tf + 1; u <= tl; ++u) {
+#pragma unroll
+                for (int q = 0; q < NG; ++q) a[q] += part[pidx(pb, r, 0, q, u)];
+            }
+        }
+        if constexpr (CF == CF_DIFFERENCE) {
+#pragma unroll
+            for (int q = 0; q < NG; ++q) a[q] = fmaf(-node.x[M::cvar(q)], wsum, a[q]);
+        }
+        post<CF, NCV>(a, cf, c);
+        if (STOCH_BLOCK_START(ks)) node.noise_block(L, r0 + tid, s0 + 1 + ks);
+        node.advance(L, Ip, r0 + tid, n, s0, ks, c);
+        float* dst = ring + ((size_t)(r0 + tid) * RS + wslot) * NCV;
+        node.write_ring(dst);
+        if (wslot < GUARD) node.write_ring(dst + (size_t)RL * NCV);  // the mirror past ring_len
+    };
+
+    const int K = L.sync_every;  // a multiple of 4
+    int since_sync = 0;
+    int bslot = (int)(s0 % RL);  // slot of the last time written before the current block
+    if (g >= 0) gather4(bslot, 0);
+    __syncthreads();
+    const int nblk = (nsteps + 3) >> 2;
+    for (int b = 0; b < nblk; ++b) {
+        const int pb = b & 1;
+        if (tid < T0) {
+            if (upd) {
+                int ws = bslot;
+#pragma unroll 1
+                for (int r = 0; r < 4; ++r) {
+                    const int ks = 4 * b + r;
+                    if (ks >= nsteps) break;
+                    ws = (ws + 1 == RL) ? 0 : ws + 1;
+                    update(ks, ws, pb, r);
+                }
+            }
+        } else if (b + 1 < nblk) {
+            int nxt = bslot + 4;  // the next block's base time
+            nxt -= nxt >= RL ? RL : 0;
+            gather4(nxt, pb ^ 1);
+        }
+        bslot += 4;
+        bslot -= bslot >= RL ? RL : 0;
+        __syncthreads();
+        since_sync += 4;
+        if (since_sync >= K) {
+            since_sync = 0;
+            cluster.sync();
+        }
+    }
+    cluster.sync();
+    if (upd) node.finish(L, Ip, r0 + tid, n, status);
+    if (rank == 0 && tid == 0) Ip->step = s_end;
+}
+
+template <class M, int CF, int SCHEME, int E, bool EXT>
+int launch_cluster_blocks_t(const tvbk_launch& L, cudaStream_t st) {
+    if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE) {
+        return -2;
+    } else {
+        auto kern = sim_kernel_cluster_blocks<M, CF, SCHEME, E, EXT>;
+        const int C = L.cluster;
+        const int R = cluster_rows(L.max_n, C);
+        const size_t smem = cluster_blocks_head(R, M::NCV, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
+        if (smem > 227 * 1024) return -1;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        if (C > 8) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return (int)e;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(L.n_inst * C), 1, 1);
+        cfg.blockDim = dim3(kClusterThreads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, kern, L);
+        return (int)e;
+    }
+}
+
+template <class M, int CF, int SCHEME, bool EXT>
+int launch_cluster_blocks(const tvbk_launch& L, cudaStream_t st) {
+    switch (L.edges_per_thread) {
+        case 8: return launch_cluster_blocks_t<M, CF, SCHEME, 8, EXT>(L, st);
+        case 16: return launch_cluster_blocks_t<M, CF, SCHEME, 16, EXT>(L, st);
+        case 32: return launch_cluster_blocks_t<M, CF, SCHEME, 32, EXT>(L, st);
+        default: return -2;
+    }
+}
+
 template <class M, int CF, int SCHEME, int E, bool PIPE, bool EXT>
 int launch_cluster_runs_t(const tvbk_launch& L, cudaStream_t st) {
     auto kern = sim_kernel_cluster_runs<M, CF, SCHEME, E, PIPE, EXT>;
@@ -517,6 +786,11 @@ int launch_cluster_p(const tvbk_launch& L, cudaStream_t st) {
 
 template <class M, int CF, int SCHEME>
 int launch_cluster(const tvbk_launch& L, cudaStream_t st) {
+    if (L.ring_layout == 1) {  // blocked edge runs on region-major rings
+        if (L.edges_per_thread <= 0 || !L.prefetch) return -2;
+        if (L.extras == 0) return launch_cluster_blocks<M, CF, SCHEME, false>(L, st);
+        return launch_cluster_blocks<M, CF, SCHEME, true>(L, st);
+    }
     if (L.edges_per_thread > 0) {  // edge runs
         if (L.extras == 0) {
             if (L.prefetch) return launch_cluster_runs<M, CF, SCHEME, true, false>(L, st);

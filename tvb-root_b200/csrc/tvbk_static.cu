@@ -93,6 +93,8 @@ extern "C" int tvbk_sim_run_static(const tvbk_launch* L, const tvbk_inst* inst, 
     if (inst->ring_len < inst->horizon + L->sync_every)
         return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: ring_len %d < horizon + sync_every", inst->ring_len);
     if (inst->step_end < inst->step) return sfail(TVBK_ERR_INVALID, "tvbk_sim_run_static: step_end < step");
+    if (L->ring_layout != 0)
+        return sfail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run_static: time-major rings only (ring_layout 0)");
 
     // scratch layout: descriptor | status | tavg_acc | bold_acc | bold_stock | aff_acc | proj_acc | ring | pre_ring
     const int64_t n = inst->n, nvoi = L->nvoi;

@@ -36,6 +36,12 @@ STATIC_SCRATCH_BYTES = 8 * 1024 * 1024
 RING_GUARD = 3
 
 
+def ring_region_stride(ring_len, ncvar):
+    """Slots per region of a region-major ring (TVBK_RING_REGION_STRIDE)."""
+    spc = 4 // ncvar
+    return -(-(ring_len + (7 if ncvar == 1 else 5)) // spc) * spc
+
+
 class Edge(ctypes.Structure):
     _fields_ = [('off', ctypes.c_int32), ('weight', ctypes.c_float)]
 
@@ -117,6 +123,7 @@ class Launch(ctypes.Structure):
         ('lanes', ctypes.c_int32),
         ('cluster', ctypes.c_int32),
         ('cluster_edges', ctypes.c_int32),
+        ('ring_layout', ctypes.c_int32),
         ('extras', ctypes.c_int32),
         ('inst_order', ctypes.c_void_p),
         ('occupancy', ctypes.c_void_p),

@@ -63,6 +63,25 @@ def ring_from_reference(buffer, step, ring_len):
     return ring
 
 
+def ring_region_major(ring, ncvar):
+    """Time-major ring (ring_len, n, ncvar) to the region-major layout of the
+    cluster kernel's blocked runs: (n, stride, ncvar), the slots past ring_len
+    mirroring slots 0, 1, ... (TVBK_RING_REGION_STRIDE / _GUARD)."""
+    ring = np.asarray(ring)
+    RL, n, ncv = ring.shape
+    RS = _lib.ring_region_stride(RL, ncvar)
+    out = np.zeros((n, RS, ncv), dtype=ring.dtype)
+    out[:, :RL] = ring.transpose(1, 0, 2)
+    g = RS - RL
+    out[:, RL:RL + g] = out[:, :g]
+    return out
+
+
+def ring_time_major(rm, ring_len):
+    """Inverse of ring_region_major."""
+    return np.ascontiguousarray(np.asarray(rm)[:, :ring_len].transpose(1, 0, 2))
+
+
 def ring_to_reference(ring, step, horizon):
     """Inverse of ring_from_reference for the times [step - horizon + 1, step]."""
     ring = np.asarray(ring)
@@ -233,7 +252,8 @@ class InstanceSpec:
 
 class Batch:
     def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
-                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True, cluster='auto'):
+                 sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True, cluster='auto',
+                 region_rings=True):
         self.lib = _lib.load()
         self.device = torch.device(device if device is not None else 'cuda')
         self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
@@ -314,6 +334,7 @@ class Batch:
         # mirrored guard slots past a shared-memory ring (prefetch 1; the split kernel has none)
         self.guard = _lib.RING_GUARD if (self.prefetch == 1 and self.ring_in_smem and V == 1) else 0
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
+        self.ring_layout = 0
         if self.cluster:
             # edge runs for the cluster CTAs when they fit; with them Difference also prefetches
             runs = self._choose_cluster_runs(dmin)
@@ -322,6 +343,13 @@ class Batch:
                 if dmin >= 1 and self.cfun_id == _lib.CFUN_IDS['Difference']:
                     self.prefetch = 1
                     self.sync_every = min(self.sync_every, dmin)
+                # blocked runs on region-major rings: four steps per gather, K a multiple of 4, <= d_min - 3
+                K4 = (min(self.sync_every, dmin - 3) // 4) * 4
+                if (region_rings and self.prefetch == 1 and K4 >= 4 and self.ncvar_gather == self.ncvar <= 2
+                        and self.cfun_id in (_lib.CFUN_IDS['Linear'], _lib.CFUN_IDS['Difference'])
+                        and self._cluster_smem(blocks=True) <= self.CLUSTER_SMEM):
+                    self.ring_layout = 1
+                    self.sync_every = K4
         self.slot_width, self._ring_len = self._choose_slots()
         self._plan()
         self.allocated = False
@@ -452,6 +480,15 @@ class Batch:
     CLUSTER_THREADS = 512
     CLUSTER_RUNS = (8, 16, 32)
 
+    def _cluster_smem(self, blocks=False):
+        """Shared memory of an edge-run cluster CTA: row pointers, the
+        double-buffered partials (of four steps for the blocked runs) and the
+        CTA's edges with room for the interleaving."""
+        R = -(-self.max_n // self.cluster)
+        nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
+        parts = 2 * (4 if blocks else 1) * self.CLUSTER_THREADS * 2 * nacc * 4
+        return -(-(R + 1) * 4 // 16) * 16 + -(-parts // 16) * 16 + 8 * (self.cluster_edges + max(self.CLUSTER_RUNS))
+
     def _choose_cluster_runs(self, dmin):
         """Edge-run length of the cluster kernel, or 0 for a warp per row: the
         smallest E of CLUSTER_RUNS whose runs cover every CTA's edges with the
@@ -464,9 +501,7 @@ class Batch:
             return 0
         C = self.cluster
         R = -(-self.max_n // C)
-        nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
-        head = -(-(R + 1) * 4 // 16) * 16 + -(-2 * self.CLUSTER_THREADS * 2 * nacc * 4 // 16) * 16
-        if head + 8 * (self.cluster_edges + max(self.CLUSTER_RUNS)) > self.CLUSTER_SMEM:
+        if self._cluster_smem() > self.CLUSTER_SMEM:
             return 0
         ahead = dmin >= 1 and self.model_id != _lib.MODEL_IDS['Sum']
         need, cap = 1, 1 << 30
@@ -535,7 +570,8 @@ class Batch:
             first = {}
             for k, s in enumerate(specs):
                 RL = self._ring_len(s)
-                init.add(('ring', k), RL * s.conn.n * self.ncvar * 4)
+                slots = _lib.ring_region_stride(RL, self.ncvar) if self.ring_layout else RL
+                init.add(('ring', k), slots * s.conn.n * self.ncvar * 4)
                 key = (_array_key(s.ring0), s.step0, RL)
                 self._ring_src[k] = first.setdefault(key, k)
         self._ring_block = init.size
@@ -664,7 +700,8 @@ class Batch:
             if V == 1:
                 src = self._ring_src[k]
                 if src == k:
-                    d['ring'] = put(('ring', k), ring_from_reference(s.ring0, s.step0, RL))
+                    r0 = ring_from_reference(s.ring0, s.step0, RL)
+                    d['ring'] = put(('ring', k), ring_region_major(r0, self.ncvar) if self.ring_layout else r0)
                 else:
                     d['ring'] = ib + init.regions[('ring', k)][0]
             elif k % V == 0:
@@ -832,6 +869,7 @@ class Batch:
         L.lanes = self.lanes
         L.cluster = self.cluster
         L.cluster_edges = self.cluster_edges
+        L.ring_layout = self.ring_layout
         L.extras = self.extras
         L.prefetch = self.prefetch
         L.max_steps = int(max_steps)
@@ -1080,6 +1118,10 @@ class Batch:
         m = self.meta[k]
         V = self.lanes
         lead = k - k % V
+        if self.ring_layout:
+            RS = _lib.ring_region_stride(m['ring_len'], self.ncvar)
+            rm = self._iview(('ring', k), torch.float32, (m['n'], RS, self.ncvar)).cpu().numpy()
+            return ring_time_major(rm, m['ring_len'])
         r = self._iview(('ring', lead), torch.float32, (m['ring_len'], m['n'], self.ncvar, V)).cpu().numpy()
         return np.ascontiguousarray(r[..., k % V])
 
@@ -1091,8 +1133,8 @@ class Batch:
     def gather_delayed(self, k, step):
         """Delayed values the coupling of `step` reads for every edge of instance k
         (read through the same address arithmetic as the kernel)."""
-        if self.lanes != 1 or self.sigma:
-            raise ValueError('gather_delayed reads single-instance rings of raw coupling variables')
+        if self.lanes != 1 or self.sigma or self.ring_layout:
+            raise ValueError('gather_delayed reads single-instance time-major rings of raw coupling variables')
         m = self.meta[k]
         conn = self.specs[k].conn
         out = torch.empty(max(conn.nnz, 1) * self.ncvar, dtype=torch.float32, device=self.device)

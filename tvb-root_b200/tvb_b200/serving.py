@@ -132,7 +132,7 @@ class SimulationServer:
         if noise_kind == _lib.NOISE_FED:
             raise NotImplementedError('the server draws device noise; use noise_source="philox"')
         plan = Batch(sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, sim.integrator.dt, sim._voi_codes,
-                     [spec], device=self.device, gather='row', allocate=False)
+                     [spec], device=self.device, gather='row', allocate=False, region_rings=False)
         # one kernel configuration per group: the components and the variant the plan chose (ring staging,
         # cluster, prefetch, sigmoid ring), so every occupant of a launch has the buffers that launch reads
         key = (sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, float(np.float32(sim.integrator.dt)),
