@@ -444,7 +444,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 // steps at a time: for the next block of four steps an edge needs its
 // source's values at four consecutive times, which sit side by side in the
 // region-major ring -- one window of three (two for one coupling variable)
-// 16-byte L2 loads instead of four scattered 8-byte loads, each of which
+// 16-byte L2 loads, the last only when the first time's slot is not on a
+// 16-byte boundary, instead of four scattered 8-byte loads, each of which
 // costs a 32-byte sector.  The window starts on a 16-byte boundary at or
 // below the first time's slot and may run past ring_len into the region's
 // guard slots, which mirror slots 0, 1, ....  The update warps advance the
@@ -568,7 +569,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
                 float win[NCH * 4];
 #pragma unroll
                 for (int c = 0; c < NCH; ++c) {
-                    const float4 t = __ldcg(src + c);
+                    // the last chunk holds times only when the window starts below the first time's slot
+                    const float4 t = (c < NCH - 1 || o != 0) ? __ldcg(src + c) : make_float4(0.f, 0.f, 0.f, 0.f);
                     win[4 * c] = t.x;
                     win[4 * c + 1] = t.y;
                     win[4 * c + 2] = t.z;

@@ -415,8 +415,11 @@ class Batch:
                 return -(-(s.conn.horizon + K) // m) * m
             return f
 
+        # ring lengths depend on a spec's horizon and size only: evaluate them once per distinct pair
+        shapes = list({(s.conn.horizon, s.conn.n): s for s in self.specs}.values())
+
         def ctas(ring_len):
-            b = (max(ring_len(s) for s in self.specs) + G) * self.max_n * self.ncvar_gather * 4
+            b = (max(ring_len(s) for s in shapes) + G) * self.max_n * self.ncvar_gather * 4
             return 0 if b > 227 * 1024 else self.SM_SMEM // (b + self.CTA_RESERVED)
 
         if not (self.ring_in_smem and self.lanes == 1 and not self.edges_per_thread and self.prefetch != 2

@@ -228,7 +228,11 @@ class ParameterSweep:
         self.run_device()
         res = {}
         if fc and any(isinstance(m, monitors_mod.Bold) for m in self.monitors):
-            res['fc'] = self.fc_device().cpu().numpy()
+            dev = self.fc_device()
+            host = torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True)   # pinned: a full-speed copy
+            host.copy_(dev, non_blocking=True)
+            torch.cuda.current_stream(dev.device).synchronize()
+            res['fc'] = host.numpy()
         outs = self.batch.outputs_host()
         proj_mons = [m for m in self.monitors if isinstance(m, monitors_mod.Projection)]
         if proj_mons and len({s.n_steps for s in self._specs}) == 1:
