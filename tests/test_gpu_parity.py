@@ -433,18 +433,19 @@ def test_kernel_variants_agree(cfun):
         sweep = {'coupling.a': np.linspace(0.5, 2.0, 8)}
         mons, length = [monitors.TemporalAverage(period=1.0)], 200.0
     out = {}
-    variants = [('row', 1, None, 0), ('row', 1, False, 0), ('row', 'auto', None, 0), ('row', 1, False, 4),
-                ('row', 1, False, 16)]
+    variants = [('row', 1, None, 0, True), ('row', 1, False, 0, True), ('row', 'auto', None, 0, True),
+                ('row', 1, False, 4, True), ('row', 1, False, 16, True), ('row', 1, False, 16, False)]
     if cfun != 'Difference':
-        variants += [('edge', 1, None, 0), ('split', 1, True, 0)]
-    for gather, lanes, smem, cluster in variants:
+        variants += [('edge', 1, None, 0, True), ('split', 1, True, 0, True)]
+    layouts = set()
+    for gather, lanes, smem, cluster, rr in variants:
         np.random.seed(11)
         sw = ParameterSweep(model=model, connectivity=Connectivity(w, L, speed=5.0), coupling=cf, integrator=integ(),
                             monitors=mons, simulation_length=length, sweep=sweep, gather=gather, lanes=lanes,
-                            ring_in_smem=smem, cluster=cluster).configure()
+                            ring_in_smem=smem, cluster=cluster, region_rings=rr).configure()
         res = sw.run(fc=False)
         assert (res['status'] == 0).all()
-        key = (gather, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster)
+        key = (gather, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster, sw.batch.ring_layout)
         if lanes == 'auto':
             assert sw.batch.lanes == 8 // sw.batch.ncvar
         if gather == 'edge':
@@ -452,11 +453,17 @@ def test_kernel_variants_agree(cfun):
         assert sw.batch.cluster == cluster
         if cluster:
             assert sw.batch.edges_per_thread in (8, 16, 32) and sw.batch.prefetch == 1, (cluster, sw.batch.edges_per_thread)
+            layouts.add(sw.batch.ring_layout)
+        if not rr:
+            assert sw.batch.ring_layout == 0
         out[key] = res
-    base = out[('row', 1, True, 0)]
+    # time-major rings (one-step edge runs) always; region-major rings (four-step blocks) where the coupling
+    # gathers the model's own coupling variables
+    assert layouts == ({0} if cfun == 'SigmoidalJansenRit' else {0, 1}), layouts
+    base = out[('row', 1, True, 0, 0)]
     for key, res in out.items():
         for mon in ('tavg', 'bold'):
-            if mon in res and key != ('row', 1, True, 0):
+            if mon in res and key != ('row', 1, True, 0, 0):
                 report('%s %s %s vs row' % (cfun, mon, key), res[mon], base[mon], 1e-5)
 
 

@@ -41,8 +41,25 @@ namespace cgx = cooperative_groups;
 
 constexpr int kClusterThreads = 512;
 constexpr int kClusterRowsPerPass = 4;
+// edges whose four-step windows a blocked-run gather thread requests together
+constexpr int kClusterBlockBatch = 2;
+// edges whose values an edge-run gather thread (one step per gather) requests together
+constexpr int kClusterRunBatch = 4;
 
 __host__ __device__ inline int cluster_rows(int n, int C) { return (n + C - 1) / C; }
+
+// CTA barrier 1 over nthreads threads (a multiple of 32), for warp-uniform
+// roles that reach it from different loops; it orders memory like
+// __syncthreads.
+__device__ __forceinline__ void cta_barrier_all(int nthreads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Cluster barrier (release on arrival, acquire on wait), in its form that
+// may be reached from different places of the code.
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
 
 // Shared memory of the edge-run variant: row pointers, then the double-buffered
 // partials ([2][threads][2][ng] floats), then the CTA's edges.
@@ -353,32 +370,51 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 
     const size_t half = (size_t)blockDim.x * 2 * NG;  // floats of one buffer of partials: [2 NG][blockDim]
     const int TB = blockDim.x;
+    // The edges go in batches of kClusterRunBatch whose loads are all issued before the first is used (one
+    // L2 round trip per batch); slots past the run's count read region 0 at time prev and add nothing.  One
+    // set of sums serves both rows of a run: at the second row's first edge (kb) the first row's sums go to
+    // partial 0.
     auto gather = [&](int prev, int buf) {
+        constexpr int BE = kClusterRunBatch;
         const int base_off = prev * slot_floats;
-        float pa[NG], pb[NG];
+        float* out = part + buf * half + g;
+        float pa[NG];
 #pragma unroll
-        for (int q = 0; q < NG; ++q) pa[q] = pb[q] = 0.0f;
+        for (int q = 0; q < NG; ++q) pa[q] = 0.0f;
 #pragma unroll
-        for (int k = 0; k < E; ++k) {
-            if (k < cnt) {
-                const int2 ed = esm[k * nrun + g];
-                float v[NG];
-                load_cg<NG>(ring + gather_addr(base_off, ed.x, ring_floats), v);
-                const float w = __int_as_float(ed.y);
-                const float wa = k < kb ? w : 0.0f, wb = k < kb ? 0.0f : w;
+        for (int k0 = 0; k0 < E; k0 += BE) {
+            if (k0 < cnt) {
+                float v[BE][NG];
+                float wv[BE];
 #pragma unroll
-                for (int q = 0; q < NG; ++q) {
-                    pa[q] = fmaf(wa, v[q], pa[q]);
-                    pb[q] = fmaf(wb, v[q], pb[q]);
+                for (int j = 0; j < BE; ++j) {
+                    const int k = k0 + j;
+                    const int2 ed = k < cnt ? esm[k * nrun + g] : make_int2(0, 0);
+                    wv[j] = __int_as_float(ed.y);
+                    load_cg<NG>(ring + gather_addr(base_off, ed.x, ring_floats), v[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < BE; ++j) {
+                    const int k = k0 + j;
+                    if (k < cnt) {
+                        if (k == kb) {
+#pragma unroll
+                            for (int q = 0; q < NG; ++q) {
+                                out[q * TB] = pa[q];
+                                pa[q] = 0.0f;
+                            }
+                        }
+#pragma unroll
+                        for (int q = 0; q < NG; ++q) pa[q] = fmaf(wv[j], v[j][q], pa[q]);
+                    }
                 }
             }
         }
-        float* out = part + buf * half + g;
+        // the last row's sums: partial 1 when the run holds a second row (partial 1 of a run without one is
+        // never read), else partial 0
+        const int h = kb < cnt ? 1 : 0;
 #pragma unroll
-        for (int q = 0; q < NG; ++q) {
-            out[q * TB] = pa[q];
-            out[(NG + q) * TB] = pb[q];
-        }
+        for (int q = 0; q < NG; ++q) out[(h * NG + q) * TB] = pa[q];
     };
     auto update = [&](int ks, int wslot, int buf) {
         const float* in = part + buf * half;
@@ -407,35 +443,52 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
     };
 
     const int K = L.sync_every;
-    int since_sync = 0;
-    int wslot = (int)(s0 % RL);  // slot of the last written time
+    const int wslot0 = (int)(s0 % RL);  // slot of the last written time
     if constexpr (PIPE) {
-        if (g >= 0) gather(wslot, 0);
+        if (g >= 0) gather(wslot0, 0);
         __syncthreads();
-    }
-    for (int ks = 0; ks < nsteps; ++ks) {
-        const int prev = wslot;
-        wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
-        if constexpr (PIPE) {
-            if (tid < T0) {
+        // The two roles run separate loops, so that the model state is not held in the gather threads'
+        // registers.  Both end every step with CTA barrier 1 over all threads and every K steps with a
+        // cluster barrier, in the same order.
+        int wslot = wslot0, since_sync = 0;
+        if (tid < T0) {
+            for (int ks = 0; ks < nsteps; ++ks) {
+                wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
                 if (upd) update(ks, wslot, ks & 1);
-            } else if (ks + 1 < nsteps) {
-                gather(wslot, (ks + 1) & 1);  // step s + 1: times <= s - d_min
+                cta_barrier_all(TB);
+                if (++since_sync == K) {
+                    since_sync = 0;
+                    cluster_barrier();
+                }
             }
-            __syncthreads();
         } else {
+            for (int ks = 0; ks < nsteps; ++ks) {
+                wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
+                if (ks + 1 < nsteps) gather(wslot, (ks + 1) & 1);  // step s + 1: times <= s - d_min
+                cta_barrier_all(TB);
+                if (++since_sync == K) {
+                    since_sync = 0;
+                    cluster_barrier();
+                }
+            }
+        }
+    } else {
+        int wslot = wslot0, since_sync = 0;
+        for (int ks = 0; ks < nsteps; ++ks) {
+            const int prev = wslot;
+            wslot = (wslot + 1 == RL) ? 0 : wslot + 1;
             gather(prev, 0);
             __syncthreads();
             if (upd) update(ks, wslot, 0);
             __syncthreads();
-        }
-        if (++since_sync == K) {
-            since_sync = 0;
-            cluster.sync();
+            if (++since_sync == K) {
+                since_sync = 0;
+                cluster.sync();
+            }
         }
     }
-    cluster.sync();
     if (upd) node.finish(L, Ip, r0 + tid, n, status);
+    cluster.sync();
     if (rank == 0 && tid == 0) Ip->step = s_end;
 }
 
@@ -550,56 +603,86 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
 
     // partial (buffer pb, step r of the block, half h, variable q) of run u
     auto pidx = [&](int pb, int r, int h, int q, int u) { return ((((pb * 4 + r) * 2 + h) * NG + q) * TB) + u; };
-    // couplings of the four steps after the time in slot st0: step r reads times (that time) + r - d
+    // couplings of the four steps after the time in slot st0: step r reads times (that time) + r - d.  The
+    // edges go in batches of BE: the windows of a batch are all requested before the first is used, so a
+    // thread waits for one L2 round trip per batch rather than one per edge.  Slots past the run's count
+    // load a harmless in-bounds window (region 0 at st0) and add nothing.  One set of sums serves both
+    // rows of a run: at the second row's first edge (kb) the first row's sums go to partial 0.
     auto gather4 = [&](int st0, int pb) {
-        float pa[4][NG], pbs[4][NG];
+        constexpr int BE = kClusterBlockBatch;
+        float pa[4][NG];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int q = 0; q < NG; ++q) pa[r][q] = pbs[r][q] = 0.0f;
+            for (int q = 0; q < NG; ++q) pa[r][q] = 0.0f;
 #pragma unroll
-        for (int k = 0; k < E; ++k) {
-            if (k < cnt) {
-                const int2 ed = esm[k * nrun + g];
-                const int d = ed.x >> 10, col = ed.x & 1023;
-                int sl = st0 - d;
-                sl += sl < 0 ? RL : 0;
-                const int a = sl & ~(SPC - 1), o = sl - a;
-                const float4* src = reinterpret_cast<const float4*>(ring + ((size_t)col * RS + a) * NG);
-                float win[NCH * 4];
+        for (int k0 = 0; k0 < E; k0 += BE) {
+            if (k0 < cnt) {
+                float4 win[BE][NCH];
+                int ov[BE];
+                float wv[BE];
 #pragma unroll
-                for (int c = 0; c < NCH; ++c) {
-                    // the last chunk holds times only when the window starts below the first time's slot
-                    const float4 t = (c < NCH - 1 || o != 0) ? __ldcg(src + c) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    win[4 * c] = t.x;
-                    win[4 * c + 1] = t.y;
-                    win[4 * c + 2] = t.z;
-                    win[4 * c + 3] = t.w;
+                for (int j = 0; j < BE; ++j) {
+                    const int k = k0 + j;
+                    const int2 ed = k < cnt ? esm[k * nrun + g] : make_int2(0, 0);
+                    const int d = ed.x >> 10, col = ed.x & 1023;
+                    int sl = st0 - d;
+                    sl += sl < 0 ? RL : 0;
+                    const int a = sl & ~(SPC - 1);
+                    ov[j] = sl - a;
+                    wv[j] = __int_as_float(ed.y);
+                    const float4* src = reinterpret_cast<const float4*>(ring + ((size_t)col * RS + a) * NG);
+#pragma unroll
+                    for (int c = 0; c < NCH; ++c)
+                        // the last chunk holds times only when the window starts below the first time's slot
+                        win[j][c] = (c < NCH - 1 || ov[j] != 0) ? __ldcg(src + c) : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
-                const float w = __int_as_float(ed.y);
-                const float wa = k < kb ? w : 0.0f, wb = k < kb ? 0.0f : w;
 #pragma unroll
-                for (int r = 0; r < 4; ++r)
+                for (int j = 0; j < BE; ++j) {
+                    const int k = k0 + j;
+                    if (k < cnt) {
+                        if (k == kb) {
 #pragma unroll
-                    for (int q = 0; q < NG; ++q) {
-                        float v;
-                        if constexpr (NG == 2) {
-                            v = o ? win[(r + 1) * 2 + q] : win[r * 2 + q];
-                        } else {
-                            v = o == 0 ? win[r] : (o == 1 ? win[r + 1] : (o == 2 ? win[r + 2] : win[r + 3]));
+                            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                                for (int q = 0; q < NG; ++q) {
+                                    part[pidx(pb, r, 0, q, g)] = pa[r][q];
+                                    pa[r][q] = 0.0f;
+                                }
                         }
-                        pa[r][q] = fmaf(wa, v, pa[r][q]);
-                        pbs[r][q] = fmaf(wb, v, pbs[r][q]);
+                        float x[NCH * 4];
+#pragma unroll
+                        for (int c = 0; c < NCH; ++c) {
+                            x[4 * c] = win[j][c].x;
+                            x[4 * c + 1] = win[j][c].y;
+                            x[4 * c + 2] = win[j][c].z;
+                            x[4 * c + 3] = win[j][c].w;
+                        }
+                        const int o = ov[j];
+                        const float w = wv[j];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+#pragma unroll
+                            for (int q = 0; q < NG; ++q) {
+                                float v;
+                                if constexpr (NG == 2) {
+                                    v = o ? x[(r + 1) * 2 + q] : x[r * 2 + q];
+                                } else {
+                                    v = o == 0 ? x[r] : (o == 1 ? x[r + 1] : (o == 2 ? x[r + 2] : x[r + 3]));
+                                }
+                                pa[r][q] = fmaf(w, v, pa[r][q]);
+                            }
                     }
+                }
             }
         }
+        // the last row's sums: partial 1 when the run holds a second row (partial 1 of a run without one is
+        // never read), else partial 0
+        const int h = kb < cnt ? 1 : 0;
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int q = 0; q < NG; ++q) {
-                part[pidx(pb, r, 0, q, g)] = pa[r][q];
-                part[pidx(pb, r, 1, q, g)] = pbs[r][q];
-            }
+            for (int q = 0; q < NG; ++q) part[pidx(pb, r, h, q, g)] = pa[r][q];
     };
     auto update = [&](int ks, int wslot, int pb, int r) {
         float a[NG], c[NCV];
@@ -626,14 +709,16 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
     };
 
     const int K = L.sync_every;  // a multiple of 4
-    int since_sync = 0;
-    int bslot = (int)(s0 % RL);  // slot of the last time written before the current block
-    if (g >= 0) gather4(bslot, 0);
+    const int bslot0 = (int)(s0 % RL);  // slot of the last time written before the first block
+    if (g >= 0) gather4(bslot0, 0);
     __syncthreads();
     const int nblk = (nsteps + 3) >> 2;
-    for (int b = 0; b < nblk; ++b) {
-        const int pb = b & 1;
-        if (tid < T0) {
+    // The two roles run separate loops, so that the model state is not held in the gather threads'
+    // registers.  Both end every block with CTA barrier 1 over all threads and every K steps with a
+    // cluster barrier, in the same order.
+    if (tid < T0) {
+        int bslot = bslot0, since_sync = 0;
+        for (int b = 0; b < nblk; ++b) {
             if (upd) {
                 int ws = bslot;
 #pragma unroll 1
@@ -641,25 +726,38 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
                     const int ks = 4 * b + r;
                     if (ks >= nsteps) break;
                     ws = (ws + 1 == RL) ? 0 : ws + 1;
-                    update(ks, ws, pb, r);
+                    update(ks, ws, b & 1, r);
                 }
             }
-        } else if (b + 1 < nblk) {
-            int nxt = bslot + 4;  // the next block's base time
-            nxt -= nxt >= RL ? RL : 0;
-            gather4(nxt, pb ^ 1);
+            bslot += 4;
+            bslot -= bslot >= RL ? RL : 0;
+            cta_barrier_all(TB);
+            since_sync += 4;
+            if (since_sync >= K) {
+                since_sync = 0;
+                cluster_barrier();
+            }
         }
-        bslot += 4;
-        bslot -= bslot >= RL ? RL : 0;
-        __syncthreads();
-        since_sync += 4;
-        if (since_sync >= K) {
-            since_sync = 0;
-            cluster.sync();
+        if (upd) node.finish(L, Ip, r0 + tid, n, status);
+    } else {
+        int bslot = bslot0, since_sync = 0;
+        for (int b = 0; b < nblk; ++b) {
+            if (b + 1 < nblk) {
+                int nxt = bslot + 4;  // the next block's base time
+                nxt -= nxt >= RL ? RL : 0;
+                gather4(nxt, (b & 1) ^ 1);
+            }
+            bslot += 4;
+            bslot -= bslot >= RL ? RL : 0;
+            cta_barrier_all(TB);
+            since_sync += 4;
+            if (since_sync >= K) {
+                since_sync = 0;
+                cluster_barrier();
+            }
         }
     }
     cluster.sync();
-    if (upd) node.finish(L, Ip, r0 + tid, n, status);
     if (rank == 0 && tid == 0) Ip->step = s_end;
 }
 

@@ -45,11 +45,16 @@ class ParameterSweep:
     same noise whichever process runs it, and results come back in the order
     of `self.instances` ('instances' in run()'s result); gather_sweep()
     reassembles the shards on one rank in global order.
+
+    region_rings: clusters of CTAs per instance keep each region's history
+    contiguous (region-major rings) when the delays allow four-step gathers;
+    False keeps the time-major ring and the one-step edge-run kernel.
     """
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
                  noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
-                 gather='auto', lanes=1, cluster='auto', stimulus=None, shard=None, instances=None):
+                 gather='auto', lanes=1, cluster='auto', stimulus=None, shard=None, instances=None,
+                 region_rings=True):
         self.model = adopt_model(model)
         self.stimulus = stimulus
         self.connectivity = adopt_connectivity(connectivity)
@@ -74,6 +79,7 @@ class ParameterSweep:
         self.gather = gather
         self.lanes = lanes
         self.cluster = cluster
+        self.region_rings = region_rings
         self.batch = None
 
     def configure(self):
@@ -150,7 +156,8 @@ class ParameterSweep:
         sim = self._sim
         return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
                      sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
-                     ring_in_smem=ring_in_smem, gather=gather, lanes=lanes, cluster=cluster)
+                     ring_in_smem=ring_in_smem, gather=gather, lanes=lanes, cluster=cluster,
+                     region_rings=self.region_rings)
 
     def projection(self, mons):
         """Sensor signals of projection monitors `mons` for all instances: one
