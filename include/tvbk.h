@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define TVBK_ABI_VERSION 2
+#define TVBK_ABI_VERSION 3
 
 /* status codes */
 #define TVBK_OK 0
@@ -56,6 +56,9 @@ extern "C" {
 #define TVBK_STATUS_UNSUPPORTED 4 /* the instance asks for something this kernel variant does not do
                                    * (AfferentCoupling on a variant other than the row kernel; a stimulus,
                                    * AfferentCoupling or projection stream with launch.extras = 0) */
+#define TVBK_STATUS_TIMEOUT 8     /* a group barrier of a cooperative launch (launch.groups > 0) waited past its
+                                   * limit (4 s), or another group's did: the launch stopped early and this
+                                   * instance's state is incomplete */
 
 /* components */
 enum {
@@ -207,7 +210,8 @@ typedef struct tvbk_launch {
                                   * shared memory) */
     int32_t cluster;             /* 0 or 1: one CTA per instance; 2..16: a thread-block cluster of that many CTAs
                                   * per instance, each owning ceil(max_n / cluster) <= 480 rows, rings read in
-                                  * place (lanes 1, row gather, rings not in shared memory) */
+                                  * place (lanes 1, row gather, rings not in shared memory).  With groups > 0,
+                                  * 2..256 CTAs per instance without a hardware cluster (see groups) */
     int32_t cluster_edges;       /* cluster kernel: edges of one CTA's rows that it stages in shared memory; a CTA
                                   * with more edges reads them from global memory (0: always global) */
     int32_t ring_layout;         /* 0: rings [ring_len][n][ncvar] (time-major).  1: region-major rings for the
@@ -218,13 +222,24 @@ typedef struct tvbk_launch {
                                   * t % ring_len, and the slots past ring_len mirror slots 0, 1, ... (every write
                                   * of a mirrored slot also writes its mirror).  Four steps' couplings are gathered
                                   * together, each edge reading its four consecutive times with 16-byte loads */
+    int32_t groups;              /* 0: cluster > 1 launches one thread-block cluster per instance.  G > 0
+                                  * (ring_layout 1 only): one cooperative launch of G x cluster CTAs, all
+                                  * resident at once (at most the SMs' resident CTAs); each group of `cluster`
+                                  * consecutive CTAs takes instances from a device-side queue in inst_order
+                                  * order (index order when NULL) until the batch is done, its CTAs kept in
+                                  * step by barriers through group_sync, each wait bounded (TVBK_STATUS_TIMEOUT).
+                                  * The instances of a batch then need not fit the GPU's thread-block clusters
+                                  * at once, and an instance may use more than 16 CTAs */
+    uint32_t* group_sync;        /* groups > 0: device scratch of TVBK_GROUP_SYNC_WORDS(groups) words, 4-byte
+                                  * aligned; tvbk_sim_run zeroes it on the launch stream before each launch */
     int32_t extras;              /* bit 0: some instance has a region stimulus; bit 1: some instance has an
                                   * AfferentCoupling monitor; bit 2: some instance has a projection stream.  0
                                   * lets the row kernel with rings in shared memory use a build without any of
                                   * them (an instance that has one then gets TVBK_STATUS_UNSUPPORTED) */
     const int32_t* inst_order;   /* device [n_inst] or NULL: CTA b advances insts[inst_order[b]] and ORs its status
                                   * bits into status[inst_order[b]] (row kernel: lanes 1, no edge split, prefetch 0
-                                  * or 1; with cluster > 1, cluster b advances insts[inst_order[b]]).  Lets one
+                                  * or 1; with cluster > 1, cluster b advances insts[inst_order[b]]; with groups > 0,
+                                  * the groups take insts[inst_order[0]], insts[inst_order[1]], ... in turn).  Lets one
                                   * launch take any subset of a batch, e.g. a window of exactly one wave of resident
                                   * CTAs, or order it, e.g. the longest instances first */
     int32_t* occupancy;          /* host pointer or NULL: when set, tvbk_sim_run launches nothing and stores there
@@ -269,6 +284,10 @@ int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weig
  * slots 0, 1, ... (a four-step read loads a 48- or 32-byte window that may
  * start just below ring_len), rounded up so that every region starts on a
  * 16-byte boundary. */
+/* Words of launch.group_sync for `groups` groups: the queue head, the abort
+ * flag, then per group an arrival counter and the claimed queue index. */
+#define TVBK_GROUP_SYNC_WORDS(groups) (2 + 2 * (groups))
+
 #define TVBK_RING_REGION_GUARD(ncvar) ((ncvar) == 1 ? 7 : 5)
 #define TVBK_RING_REGION_STRIDE(ring_len, ncvar) \
     ((((ring_len) + TVBK_RING_REGION_GUARD(ncvar)) + (4 / (ncvar)) - 1) / (4 / (ncvar)) * (4 / (ncvar)))

@@ -35,7 +35,7 @@ def test_every_declared_function_is_exported_and_bound():
 
 def test_struct_sizes_and_version():
     lib = _lib.load()
-    assert lib.tvbk_abi_version() == 2
+    assert lib.tvbk_abi_version() == 3
     assert lib.tvbk_sizeof(0) == ctypes.sizeof(_lib.Inst)
     assert lib.tvbk_sizeof(1) == ctypes.sizeof(_lib.Launch)
     assert lib.tvbk_sizeof(2) == 8
@@ -99,3 +99,32 @@ def test_argument_errors_are_status_codes():
     with pytest.raises(_lib.TvbkError):
         _lib.idelays(np.full((2, 2), 10.0), -1.0, 0.1)
     assert lib.tvbk_fc(None, 1, 10, 4, None, None) == _lib.TVBK_ERR_INVALID
+
+
+def test_group_launch_arguments_are_checked():
+    """launch.groups (cooperative launch of groups of CTAs per instance) is
+    refused without region-major rings or a 4-byte aligned group_sync, and
+    allows up to 256 CTAs per instance; nothing is dereferenced or launched."""
+    lib = _lib.load()
+    L = _lib.Launch()
+    L.model, L.cfun, L.scheme = _lib.MODEL_IDS['ReducedWongWang'], _lib.CFUN_IDS['Linear'], 0
+    L.insts, L.status, L.n_inst = 16, 16, 1
+    L.max_n, L.sync_every, L.max_steps, L.dt = 68, 4, 10, 0.1
+    L.groups, L.cluster, L.ring_layout = 2, 2, 0
+    L.group_sync = 64
+    assert lib.tvbk_sim_run(ctypes.byref(L), None) == _lib.TVBK_ERR_INVALID
+    assert b'groups' in lib.tvbk_last_error()
+    L.ring_layout, L.group_sync = 1, None
+    assert lib.tvbk_sim_run(ctypes.byref(L), None) == _lib.TVBK_ERR_INVALID
+    assert b'group_sync' in lib.tvbk_last_error()
+    L.group_sync = 66
+    assert lib.tvbk_sim_run(ctypes.byref(L), None) == _lib.TVBK_ERR_INVALID
+    assert b'aligned' in lib.tvbk_last_error()
+    L.group_sync, L.cluster = 64, 300
+    assert lib.tvbk_sim_run(ctypes.byref(L), None) == _lib.TVBK_ERR_INVALID
+    assert b'0..256' in lib.tvbk_last_error()
+    L.groups = 0
+    L.cluster = 20
+    assert lib.tvbk_sim_run(ctypes.byref(L), None) == _lib.TVBK_ERR_INVALID
+    assert b'0..16' in lib.tvbk_last_error()
+

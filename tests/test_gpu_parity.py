@@ -433,37 +433,46 @@ def test_kernel_variants_agree(cfun):
         sweep = {'coupling.a': np.linspace(0.5, 2.0, 8)}
         mons, length = [monitors.TemporalAverage(period=1.0)], 200.0
     out = {}
-    variants = [('row', 1, None, 0, True), ('row', 1, False, 0, True), ('row', 'auto', None, 0, True),
-                ('row', 1, False, 4, True), ('row', 1, False, 16, True), ('row', 1, False, 16, False)]
+    variants = [('row', 1, None, 0, True, 'auto'), ('row', 1, False, 0, True, 'auto'),
+                ('row', 'auto', None, 0, True, 'auto'), ('row', 1, False, 4, True, 'auto'),
+                ('row', 1, False, 16, True, 'auto'), ('row', 1, False, 16, False, 'auto'),
+                ('row', 1, False, 4, True, True), ('row', 1, False, 'auto', True, 'auto')]
     if cfun != 'Difference':
-        variants += [('edge', 1, None, 0, True), ('split', 1, True, 0, True)]
-    layouts = set()
-    for gather, lanes, smem, cluster, rr in variants:
+        variants += [('edge', 1, None, 0, True, 'auto'), ('split', 1, True, 0, True, 'auto')]
+    layouts, grouped = set(), set()
+    for gather, lanes, smem, cluster, rr, groups in variants:
         np.random.seed(11)
         sw = ParameterSweep(model=model, connectivity=Connectivity(w, L, speed=5.0), coupling=cf, integrator=integ(),
                             monitors=mons, simulation_length=length, sweep=sweep, gather=gather, lanes=lanes,
-                            ring_in_smem=smem, cluster=cluster, region_rings=rr).configure()
+                            ring_in_smem=smem, cluster=cluster, region_rings=rr, groups=groups).configure()
         res = sw.run(fc=False)
         assert (res['status'] == 0).all()
-        key = (gather, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster, sw.batch.ring_layout)
+        key = (gather, lanes, smem, cluster, rr, groups, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster,
+               sw.batch.ring_layout, sw.batch.groups)
         if lanes == 'auto':
             assert sw.batch.lanes == 8 // sw.batch.ncvar
         if gather == 'edge':
             assert sw.batch.edges_per_thread > 0
-        assert sw.batch.cluster == cluster
-        if cluster:
+        if cluster != 'auto':
+            assert sw.batch.cluster == cluster
+        if groups is True:
+            grouped.add((sw.batch.groups, sw.batch.cluster))
+        if sw.batch.cluster:
             assert sw.batch.edges_per_thread in (8, 16, 32) and sw.batch.prefetch == 1, (cluster, sw.batch.edges_per_thread)
             layouts.add(sw.batch.ring_layout)
         if not rr:
             assert sw.batch.ring_layout == 0
         out[key] = res
     # time-major rings (one-step edge runs) always; region-major rings (four-step blocks) where the coupling
-    # gathers the model's own coupling variables
+    # gathers the model's own coupling variables, there also cooperative groups (all 8 instances at once)
     assert layouts == ({0} if cfun == 'SigmoidalJansenRit' else {0, 1}), layouts
-    base = out[('row', 1, True, 0, 0)]
+    assert grouped == ({(0, 4)} if cfun == 'SigmoidalJansenRit' else {(8, 4)}), grouped
+    bkey = [k for k in out if k[:6] == ('row', 1, None, 0, True, 'auto')][0]
+    assert bkey[7] and bkey[8] == 0  # the row kernel with rings in shared memory
+    base = out[bkey]
     for key, res in out.items():
         for mon in ('tavg', 'bold'):
-            if mon in res and key != ('row', 1, True, 0, 0):
+            if mon in res and key != bkey:
                 report('%s %s %s vs row' % (cfun, mon, key), res[mon], base[mon], 1e-5)
 
 

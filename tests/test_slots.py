@@ -59,3 +59,41 @@ def test_batch_pads_the_ring_and_keeps_two_ctas_per_sm():
     assert b.guard == _lib.RING_GUARD
     assert 228 * 1024 // ((RL + b.guard) * n * 4 + 1024) == 2
     assert 4 <= b.sync_every <= c.min_delay
+
+
+def test_large_network_batches_plan_cooperative_groups():
+    """Region-major Epileptor 998 batches plan one cooperative launch of
+    groups: 16 uneven instances on 9 groups of 16 CTAs (144 of 148 SMs, where
+    thread-block clusters of 16 fit 7 at a time), a single instance on 64
+    CTAs; an explicit cluster or groups=False keeps thread-block clusters."""
+    from tvb_b200 import _lib, coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.engine import Batch
+    from tvb_b200.sweep import ParameterSweep
+    w, L = synthetic.connectome(998, 0.10, 5.0, 300.0, seed=4)
+    x0 = np.random.default_rng(14).uniform(-2.4, -1.6, (16, 998))
+
+    def plan(ni, uneven, **kw):
+        sweep = {'model.x0': x0[:ni]}
+        if uneven:
+            sweep['simulation_length'] = np.linspace(20.0, 200.0, ni)
+        sw = ParameterSweep(model=models.Epileptor(), connectivity=Connectivity(w, L, speed=3.0),
+                            coupling=coupling.Difference(), integrator=integrators.HeunDeterministic(dt=0.05),
+                            monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=100.0, sweep=sweep,
+                            device='cpu').configure()
+        sim = sw._sim
+        return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, sw._noise_kind, sw.integrator.dt, sim._voi_codes,
+                     sw._specs, device='cpu', allocate=False, **kw)
+
+    b = plan(16, True)
+    assert (b.ring_layout, b.groups, b.cluster) == (1, 9, 16) and b.edges_per_thread == 16
+    assert b.sync_every % 4 == 0 and 4 <= b.sync_every
+    assert _lib.group_sync_words(b.groups) == 20
+    b = plan(1, False)
+    assert (b.groups, b.cluster) == (1, 64) and b.edges_per_thread in (8, 16, 32)
+    b = plan(16, True, cluster=16)
+    assert (b.groups, b.cluster, b.ring_layout) == (0, 16, 1)
+    b = plan(16, True, groups=False)
+    assert (b.groups, b.cluster) == (0, 16)
+    b = plan(16, True, groups=4)
+    assert b.groups == 4 and b.groups * b.cluster <= 148

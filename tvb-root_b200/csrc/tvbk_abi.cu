@@ -220,8 +220,13 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
                     "one step at a time (prefetch 0, lanes 1, edges_per_thread 0, cluster 0)");
     if (L->ring_layout < 0 || L->ring_layout > 1 || (L->ring_layout == 1 && L->cluster <= 1))
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: ring_layout 1 (region-major) applies to clusters only");
-    if (L->cluster < 0 || L->cluster > 16)
-        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster %d out of 0..16", L->cluster);
+    if (L->groups < 0 || (L->groups > 0 && (L->ring_layout != 1 || !L->group_sync)))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: groups > 0 (cooperative launch) needs ring_layout 1 and "
+                    "group_sync");
+    if (L->groups > 0 && (reinterpret_cast<uintptr_t>(L->group_sync) & 3) != 0)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: group_sync is not 4-byte aligned");
+    if (L->cluster < 0 || L->cluster > (L->groups > 0 ? 256 : 16))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster %d out of 0..%d", L->cluster, L->groups > 0 ? 256 : 16);
     if (L->cluster > 1) {
         if (L->lanes > 1 || L->ring_in_smem)
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster per instance reads its rings in place "
@@ -312,6 +317,11 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         smem = (size_t)b;
     }
     cudaStream_t st = (cudaStream_t)stream;
+    if (L->groups > 0) {
+        // the queue head, the abort flag and every group's barrier counter start from zero
+        const cudaError_t e = cudaMemsetAsync(L->group_sync, 0, sizeof(uint32_t) * TVBK_GROUP_SYNC_WORDS(L->groups), st);
+        if (e != cudaSuccess) return cuda_fail(e, "tvbk_sim_run group_sync");
+    }
     int rc;
     switch (L->model) {
         case TVBK_MODEL_G2D: rc = tvbk::launch_g2d(*L, st, smem); break;
@@ -321,6 +331,9 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         default: rc = tvbk::launch_sum(*L, st, smem); break;
     }
     if (rc == -1) return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: instance too large for this kernel variant");
+    if (rc == -4)
+        return fail(TVBK_ERR_TOO_LARGE, "tvbk_sim_run: %d groups x %d CTAs are more than the GPU holds at once",
+                    L->groups, L->cluster);
     if (rc == -2)
         return fail(TVBK_ERR_UNSUPPORTED, "tvbk_sim_run: model %d / coupling %d / scheme %d not built", L->model,
                     L->cfun, L->scheme);

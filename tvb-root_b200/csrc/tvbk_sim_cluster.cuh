@@ -61,6 +61,48 @@ __device__ __forceinline__ void cluster_barrier() {
     asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
 }
 
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Longest wait of one group barrier (all CTAs of a cooperative launch are
+// resident, so a wait this long means the launch cannot go on).
+constexpr uint64_t kGroupWaitNs = 4000000000ull;
+
+// Group barrier, one thread per CTA: arrive on the group's counter, then wait
+// until it reaches `target` (the group's CTAs x the barriers passed so far).
+// Returns 0 when the launch is abandoned: the abort flag is set, or this wait
+// ran past kGroupWaitNs (then this thread sets the flag, and every other wait
+// of the launch returns 0 at its next poll).
+__device__ __forceinline__ int group_arrive_wait(uint32_t* count, uint32_t target, uint32_t* abort_flag) {
+    __threadfence();  // this CTA's ring writes, ordered before the arrival by the CTA barrier before the call
+    atomicAdd(count, 1u);
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
+        if ((int32_t)(ld_acquire_gpu(count) - target) >= 0) break;
+        if (ld_acquire_gpu(abort_flag) != 0u) return 0;
+        if (globaltimer_ns() - t0 > kGroupWaitNs) {
+            atomicExch(abort_flag, 1u);
+            return 0;
+        }
+        __nanosleep(32);
+    }
+    __threadfence();
+    return 1;
+}
+
 // Shared memory of the edge-run variant: row pointers, then the double-buffered
 // partials ([2][threads][2][ng] floats), then the CTA's edges.
 __host__ __device__ inline size_t cluster_runs_head_rp(int R) { return ((size_t)(R + 1) * 4 + 15) / 16 * 16; }
@@ -507,18 +549,20 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 // of block b + 1 reads times up to 7 - d_min past the last time written
 // before block b, so it needs d_min >= 7 and a cluster barrier interval
 // K <= d_min - 3, a multiple of 4 (the windows start on block boundaries).
-template <class M, int CF, int SCHEME, int E, bool EXT = true>
-__global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(const tvbk_launch L) {
+//
+// blocked_instance runs one instance's launch window on the C CTAs of the
+// instance (this CTA is `rank`); sync() is the barrier between those CTAs
+// (every K steps and at the end), which returns false when the launch is
+// being abandoned -- then so does blocked_instance.
+template <class M, int CF, int SCHEME, int E, bool EXT, class Sync>
+__device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int inst, const int C, const int rank,
+                                                 Sync& sync) {
     static_assert(CF == CF_LINEAR || CF == CF_DIFFERENCE, "blocked runs: Linear or Difference coupling");
     constexpr int NCV = M::NCV;
     constexpr int NG = NCV;
     constexpr int SPC = 4 / NG;              // slots per 16-byte chunk
     constexpr int NCH = NG == 2 ? 3 : 2;     // 16-byte chunks per four-step window
     extern __shared__ __align__(16) unsigned char sm[];
-    cgx::cluster_group cluster = cgx::this_cluster();
-    const int C = (int)cluster.num_blocks();
-    const int rank = (int)cluster.block_rank();
-    const int inst = L.inst_order != nullptr ? L.inst_order[blockIdx.x / C] : (int)(blockIdx.x / C);
     tvbk_inst* __restrict__ Ip = L.insts + inst;
     int32_t* status = L.status + inst;
     const int n = Ip->n;
@@ -529,7 +573,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
     constexpr int GUARD = TVBK_RING_REGION_GUARD(NG);
     const int64_t s0 = Ip->step;
     const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
-    if (s0 >= s_end) return;  // uniform over the cluster
+    if (s0 >= s_end) return true;  // uniform over the instance's CTAs
     const int nsteps = (int)(s_end - s0);
     const int tid = threadIdx.x;
     const int TB = blockDim.x;
@@ -714,8 +758,9 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
     __syncthreads();
     const int nblk = (nsteps + 3) >> 2;
     // The two roles run separate loops, so that the model state is not held in the gather threads'
-    // registers.  Both end every block with CTA barrier 1 over all threads and every K steps with a
-    // cluster barrier, in the same order.
+    // registers.  Both end every block with CTA barrier 1 over all threads and every K steps with sync(),
+    // in the same order, and both see the same sync() results.
+    bool ok = true;
     if (tid < T0) {
         int bslot = bslot0, since_sync = 0;
         for (int b = 0; b < nblk; ++b) {
@@ -735,7 +780,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
             since_sync += 4;
             if (since_sync >= K) {
                 since_sync = 0;
-                cluster_barrier();
+                if (!sync()) {
+                    ok = false;
+                    break;
+                }
             }
         }
         if (upd) node.finish(L, Ip, r0 + tid, n, status);
@@ -753,12 +801,75 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
             since_sync += 4;
             if (since_sync >= K) {
                 since_sync = 0;
-                cluster_barrier();
+                if (!sync()) {
+                    ok = false;
+                    break;
+                }
             }
         }
     }
-    cluster.sync();
+    if (!ok || !sync()) return false;
     if (rank == 0 && tid == 0) Ip->step = s_end;
+    return true;
+}
+
+// One thread-block cluster of C CTAs per instance (cluster b takes instance
+// inst_order[b], or b); the cluster barrier keeps its CTAs in step.
+template <class M, int CF, int SCHEME, int E, bool EXT = true>
+__global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(const tvbk_launch L) {
+    cgx::cluster_group cluster = cgx::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int inst = L.inst_order != nullptr ? L.inst_order[blockIdx.x / C] : (int)(blockIdx.x / C);
+    auto sync = []() {
+        cluster_barrier();
+        return true;
+    };
+    blocked_instance<M, CF, SCHEME, E, EXT>(L, inst, C, (int)cluster.block_rank(), sync);
+}
+
+// Cooperative form (launch.groups = G > 0): G x C CTAs, all resident at once.
+// CTAs gC .. gC + C - 1 form group g, which claims queue positions j = 0, 1,
+// ... from a device counter (rank 0 claims, the others read the claim after a
+// group barrier) and runs instance inst_order[j] (or j) with blocked_instance,
+// until the queue is empty.  Thread-block clusters hold at most 16 CTAs and
+// only as many of them run at once as the GPCs fit (7 clusters of 16 on 148
+// SMs); groups fill every SM and take any C.  The group barrier is a counter
+// in global memory with a bounded wait; a barrier that gives up abandons the
+// launch, and every instance in flight gets TVBK_STATUS_TIMEOUT.
+template <class M, int CF, int SCHEME, int E, bool EXT = true>
+__global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_group_blocks(const tvbk_launch L) {
+    __shared__ int s_ok, s_next;
+    const int C = L.cluster;
+    const int grp = (int)blockIdx.x / C, rank = (int)blockIdx.x % C;
+    uint32_t* const queue = L.group_sync;
+    uint32_t* const abort_flag = L.group_sync + 1;
+    uint32_t* const count = L.group_sync + 2 + grp;
+    uint32_t* const claim = L.group_sync + 2 + L.groups + grp;
+    uint32_t target = 0;
+    int inst = -1;
+    auto sync = [&]() -> bool {
+        target += (uint32_t)C;
+        cta_barrier_all((int)blockDim.x);
+        if (threadIdx.x == 0) {
+            const int r = group_arrive_wait(count, target, abort_flag);
+            if (!r && inst >= 0) atomicOr(L.status + inst, TVBK_STATUS_TIMEOUT);
+            s_ok = r;
+        }
+        cta_barrier_all((int)blockDim.x);
+        return s_ok != 0;
+    };
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) st_release_gpu(claim, atomicAdd(queue, 1u));
+        if (!sync()) return;
+        if (threadIdx.x == 0) s_next = (int)ld_acquire_gpu(claim);
+        cta_barrier_all((int)blockDim.x);
+        const int j = s_next;
+        if (j >= L.n_inst) return;
+        inst = L.inst_order != nullptr ? L.inst_order[j] : j;
+        if (!blocked_instance<M, CF, SCHEME, E, EXT>(L, inst, C, rank, sync)) return;
+        // every CTA of the group has read the claim and is done with its shared memory before the next claim
+        if (!sync()) return;
+    }
 }
 
 template <class M, int CF, int SCHEME, int E, bool EXT>
@@ -794,8 +905,50 @@ int launch_cluster_blocks_t(const tvbk_launch& L, cudaStream_t st) {
     }
 }
 
+template <class M, int CF, int SCHEME, int E, bool EXT>
+int launch_group_blocks_t(const tvbk_launch& L, cudaStream_t st) {
+    if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE) {
+        return -2;
+    } else {
+        auto kern = sim_kernel_group_blocks<M, CF, SCHEME, E, EXT>;
+        const int C = L.cluster;
+        const int R = cluster_rows(L.max_n, C);
+        const size_t smem = cluster_blocks_head(R, M::NCV, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
+        if (smem + 64 > 227 * 1024) return -1;  // 64: the kernel's own shared words
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+        // every CTA must be resident at once: at most (CTAs per SM) x SMs
+        int dev = 0, sms = 0, per_sm = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kClusterThreads, smem);
+        if (e != cudaSuccess) return (int)e;
+        if ((int64_t)L.groups * C > (int64_t)per_sm * sms) return -4;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(L.groups * C), 1, 1);
+        cfg.blockDim = dim3(kClusterThreads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, kern, L);
+        return (int)e;
+    }
+}
+
 template <class M, int CF, int SCHEME, bool EXT>
 int launch_cluster_blocks(const tvbk_launch& L, cudaStream_t st) {
+    if (L.groups > 0) {
+        switch (L.edges_per_thread) {
+            case 8: return launch_group_blocks_t<M, CF, SCHEME, 8, EXT>(L, st);
+            case 16: return launch_group_blocks_t<M, CF, SCHEME, 16, EXT>(L, st);
+            case 32: return launch_group_blocks_t<M, CF, SCHEME, 32, EXT>(L, st);
+            default: return -2;
+        }
+    }
     switch (L.edges_per_thread) {
         case 8: return launch_cluster_blocks_t<M, CF, SCHEME, 8, EXT>(L, st);
         case 16: return launch_cluster_blocks_t<M, CF, SCHEME, 16, EXT>(L, st);

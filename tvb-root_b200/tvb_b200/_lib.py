@@ -20,6 +20,7 @@ TVBK_ERR_TOO_LARGE = -4
 TVBK_STATUS_NONFINITE = 1
 TVBK_STATUS_DEGREE = 2
 TVBK_STATUS_UNSUPPORTED = 4
+TVBK_STATUS_TIMEOUT = 8
 
 MODEL_IDS = {'Generic2dOscillator': 0, 'JansenRit': 1, 'ReducedWongWang': 2, 'Epileptor': 3, 'Sum': 4}
 CFUN_IDS = {'Linear': 0, 'Difference': 1, 'SigmoidalJansenRit': 2, 'Sigmoidal': 3, 'HyperbolicTangent': 4,
@@ -34,6 +35,11 @@ MAX_VOI = 8
 STATIC_SCRATCH_BYTES = 8 * 1024 * 1024
 # mirrored slots past the end of a ring staged in shared memory with prefetch = 1 (TVBK_RING_GUARD)
 RING_GUARD = 3
+
+
+def group_sync_words(groups):
+    """Words of launch.group_sync for `groups` groups (TVBK_GROUP_SYNC_WORDS)."""
+    return 2 + 2 * groups
 
 
 def ring_region_stride(ring_len, ncvar):
@@ -124,6 +130,8 @@ class Launch(ctypes.Structure):
         ('cluster', ctypes.c_int32),
         ('cluster_edges', ctypes.c_int32),
         ('ring_layout', ctypes.c_int32),
+        ('groups', ctypes.c_int32),
+        ('group_sync', ctypes.c_void_p),
         ('extras', ctypes.c_int32),
         ('inst_order', ctypes.c_void_p),
         ('occupancy', ctypes.c_void_p),

@@ -253,7 +253,7 @@ class InstanceSpec:
 class Batch:
     def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
                  sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True, cluster='auto',
-                 region_rings=True):
+                 region_rings=True, groups='auto'):
         self.lib = _lib.load()
         self.device = torch.device(device if device is not None else 'cuda')
         self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
@@ -333,6 +333,8 @@ class Batch:
                 raise ValueError('the edge-parallel gather does not apply to this batch')
         # mirrored guard slots past a shared-memory ring (prefetch 1; the split kernel has none)
         self.guard = _lib.RING_GUARD if (self.prefetch == 1 and self.ring_in_smem and V == 1) else 0
+        # an explicit cluster above 16 CTAs per instance needs cooperative groups
+        self._cluster_max = 256 if (groups is not False and groups not in (0, None, 'off', 'auto')) else 16
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
         self.ring_layout = 0
         if self.cluster:
@@ -350,6 +352,12 @@ class Batch:
                         and self._cluster_smem(blocks=True) <= self.CLUSTER_SMEM):
                     self.ring_layout = 1
                     self.sync_every = K4
+        self.groups = 0
+        if self.ring_layout == 1:
+            self._choose_groups(groups, cluster, dmin)
+        if self.cluster > 16 and not self.groups:
+            raise ValueError('%d CTAs per instance need cooperative groups, which need region-major rings '
+                             '(Linear or Difference coupling, ncvar <= 2, smallest delay >= 7 steps)' % self.cluster)
         self.slot_width, self._ring_len = self._choose_slots()
         self._plan()
         self.allocated = False
@@ -463,9 +471,9 @@ class Batch:
                 return 0, 0
         else:
             C = int(cluster)
-            if not able or not 2 <= C <= 16:
-                raise ValueError('a cluster of 2..16 CTAs per instance needs rings in place, the row gather and '
-                                 'one instance per group')
+            if not able or not 2 <= C <= self._cluster_max:
+                raise ValueError('a cluster of 2..16 CTAs per instance (2..256 with groups=True) needs rings in '
+                                 'place, the row gather and one instance per lane group')
         C = max(C, -(-self.max_n // self.CLUSTER_MAX_ROWS))
         R = -(-self.max_n // C)
         nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
@@ -482,6 +490,72 @@ class Batch:
 
     CLUSTER_THREADS = 512
     CLUSTER_RUNS = (8, 16, 32)
+    GROUP_SIZES = (8, 12, 16, 18, 20, 24, 32, 48, 64)
+
+    def _sm_count(self):
+        if self.device.type == 'cuda' and torch.cuda.is_available():
+            return torch.cuda.get_device_properties(self.device).multi_processor_count
+        return 148
+
+    def _cluster_edges_for(self, C):
+        """Largest edge count of one CTA's rows with C CTAs per instance."""
+        R = -(-self.max_n // C)
+        emax = 0
+        for s in self.specs:
+            rp = s.conn.row_ptr
+            n = s.conn.n
+            for r in range(C):
+                lo = min(n, r * R)
+                hi = min(n, lo + R)
+                emax = max(emax, int(rp[hi] - rp[lo]))
+        return emax
+
+    def _choose_groups(self, groups, cluster, dmin):
+        """Cooperative groups (launch.groups) instead of thread-block clusters
+        for blocked runs on region-major rings.  groups=True keeps the chosen
+        CTAs per instance; 'auto' (with cluster='auto') picks C from
+        GROUP_SIZES and G = min(SMs // C, instances) groups, minimising the
+        longest-processing-time makespan of the instances' lengths on G groups
+        times (1/C + 1/64): the gather of one step spreads over C CTAs, and a
+        part of the step (the update warps, the barriers) does not shrink with
+        C.  The device queue hands the instances out longest first, which is
+        that schedule.  An int caps G.  False (or an explicit cluster with
+        'auto') keeps thread-block clusters."""
+        if groups is False or groups in (0, None, 'off') or (groups == 'auto' and cluster != 'auto'):
+            return
+        sms = self._sm_count()
+        lengths = sorted((s.n_steps for s in self.specs), reverse=True)
+        keep = (self.cluster, self.cluster_edges, self.edges_per_thread)
+
+        def makespan(G):
+            loads = [0] * G
+            for L in lengths:
+                i = loads.index(min(loads))
+                loads[i] += L
+            return max(loads)
+
+        sizes = self.GROUP_SIZES if cluster == 'auto' else [self.cluster]
+        cap = int(groups) if (isinstance(groups, int) and not isinstance(groups, bool)) else None
+        best = None
+        for C in sizes:
+            G = min(sms // C, len(self.specs), cap or sms)
+            if G < 1 or -(-self.max_n // C) > self.CLUSTER_MAX_ROWS:
+                continue
+            edges = self._cluster_edges_for(C)
+            self.cluster, self.cluster_edges = C, edges
+            runs = self._choose_cluster_runs(dmin)
+            self.edges_per_thread = runs
+            fits = runs and self._cluster_smem(blocks=True) + 64 <= self.CLUSTER_SMEM
+            self.cluster, self.cluster_edges, self.edges_per_thread = keep
+            if not fits:
+                continue
+            est = makespan(G) * (1.0 / C + 1.0 / 64)
+            if best is None or est < best[0] * (1 - 1e-9):
+                best = (est, C, G, edges, runs)
+        if best is None:
+            return
+        _, C, G, edges, runs = best
+        self.cluster, self.cluster_edges, self.edges_per_thread, self.groups = C, edges, runs, G
 
     def _cluster_smem(self, blocks=False):
         """Shared memory of an edge-run cluster CTA: row pointers, the
@@ -795,6 +869,10 @@ class Batch:
         if self.cluster and len(set(lengths.tolist())) > 1:
             order = np.argsort(-lengths, kind='stable').astype(np.int32)
             self._longest_first = torch.as_tensor(order, device=dev)
+        # cooperative groups: queue head, abort flag, per-group barrier counters and claims (zeroed by the
+        # library before each launch)
+        self._group_sync = (torch.zeros(_lib.group_sync_words(self.groups), dtype=torch.int32, device=dev)
+                            if self.groups else None)
 
     def _upload_rings(self, ring_up):
         """Host-to-device copy of each distinct initial ring, then device copies
@@ -873,13 +951,15 @@ class Batch:
         L.cluster = self.cluster
         L.cluster_edges = self.cluster_edges
         L.ring_layout = self.ring_layout
+        L.groups = self.groups
+        L.group_sync = self._group_sync.data_ptr() if self.groups else None
         L.extras = self.extras
         L.prefetch = self.prefetch
         L.max_steps = int(max_steps)
         L.dt = self.dt
         if self.cluster and getattr(self, "_longest_first", None) is not None:
-            # clusters dispatch in launch order: the longest instances start first, so that the batch's
-            # last steps do not run one long instance alone
+            # clusters dispatch in launch order (groups take the queue in this order): the longest instances
+            # start first, so that the batch's last steps do not run one long instance alone
             L.inst_order = self._longest_first.data_ptr()
         return L
 

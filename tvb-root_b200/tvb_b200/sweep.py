@@ -49,12 +49,16 @@ class ParameterSweep:
     region_rings: clusters of CTAs per instance keep each region's history
     contiguous (region-major rings) when the delays allow four-step gathers;
     False keeps the time-major ring and the one-step edge-run kernel.
+    groups: with region-major rings, 'auto' (and cluster='auto') runs the
+    batch as one cooperative launch of groups of CTAs that take instances
+    from a device queue, choosing the CTAs per instance; True also with an
+    explicit cluster; False keeps thread-block clusters.
     """
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
                  noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
                  gather='auto', lanes=1, cluster='auto', stimulus=None, shard=None, instances=None,
-                 region_rings=True):
+                 region_rings=True, groups='auto'):
         self.model = adopt_model(model)
         self.stimulus = stimulus
         self.connectivity = adopt_connectivity(connectivity)
@@ -80,6 +84,7 @@ class ParameterSweep:
         self.lanes = lanes
         self.cluster = cluster
         self.region_rings = region_rings
+        self.groups = groups
         self.batch = None
 
     def configure(self):
@@ -157,7 +162,7 @@ class ParameterSweep:
         return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
                      sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
                      ring_in_smem=ring_in_smem, gather=gather, lanes=lanes, cluster=cluster,
-                     region_rings=self.region_rings)
+                     region_rings=self.region_rings, groups=self.groups)
 
     def projection(self, mons):
         """Sensor signals of projection monitors `mons` for all instances: one
