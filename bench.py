@@ -468,6 +468,8 @@ def large_network_leg(steps, warmup, local, length_scale=1.0, gather='auto', clu
     return {'value': float(steps_total * EPI_N / t), 'unit': UNIT, 'ms_per_step': 1e3 * t, 'steps': steps,
             'warmup': warmup, 'instances': n_inst, 'regions': EPI_N, 'edge_runs': b.edges_per_thread, 'nnz': int(sw._sim._conn.nnz), 'dt_ms': EPI_DT,
             'lengths_ms': lengths.tolist(), 'cluster_ctas_per_instance': b.cluster, 'sync_every': b.sync_every,
+            'launch': ('cooperative, %d groups of %d CTAs' % (b.groups, b.cluster) if b.groups
+                       else 'thread-block clusters of %d CTAs' % b.cluster),
             'nonfinite_instances': int((b.status() != 0).sum()), 'gpu_launches': steps * b.last_launches}
 
 
@@ -480,7 +482,7 @@ def run_large_network(args, rank, local):
             'config': {'workload': 'epileptor_998r_16i_uneven_2-20s', 'instances': leg['instances'], 'regions': EPI_N,
                        'nnz': leg['nnz'], 'dt_ms': EPI_DT, 'lengths_ms': leg['lengths_ms'],
                        'cluster_ctas_per_instance': leg['cluster_ctas_per_instance'],
-                       'sync_every': leg['sync_every']},
+                       'sync_every': leg['sync_every'], 'launch': leg['launch']},
             'nonfinite_instances': leg['nonfinite_instances'], 'gpu_launches': leg['gpu_launches']}
     if args.check_ms > 0:
         line['error_vs_fp64_oracle'] = large_network_error(args.check_ms, os.cpu_count() or 1)
