@@ -221,7 +221,9 @@ typedef struct tvbk_launch {
                                   * [r][TVBK_RING_REGION_STRIDE(ring_len, ncvar)][ncvar], time t in slot
                                   * t % ring_len, and the slots past ring_len mirror slots 0, 1, ... (every write
                                   * of a mirrored slot also writes its mirror).  Four steps' couplings are gathered
-                                  * together, each edge reading its four consecutive times with 16-byte loads */
+                                  * together, each edge reading its four consecutive times with 32-byte loads;
+                                  * each instance's ring must be 32-byte aligned (else the instance is not
+                                  * advanced and gets TVBK_STATUS_UNSUPPORTED) */
     int32_t groups;              /* 0: cluster > 1 launches one thread-block cluster per instance.  G > 0
                                   * (ring_layout 1 only): one cooperative launch of G x cluster CTAs, all
                                   * resident at once (at most the SMs' resident CTAs); each group of `cluster`
@@ -279,18 +281,19 @@ int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weig
  * in a row take one ring address per edge (address + r slots, r <= 3). */
 #define TVBK_RING_GUARD 3
 
-/* Region-major rings (launch.ring_layout = 1): slots per region -- the
- * ring_len slots, then a guard of 5 (ncvar 2) or 7 (ncvar 1) slots mirroring
- * slots 0, 1, ... (a four-step read loads a 48- or 32-byte window that may
- * start just below ring_len), rounded up so that every region starts on a
- * 16-byte boundary. */
 /* Words of launch.group_sync for `groups` groups: the queue head, the abort
  * flag, then per group an arrival counter and the claimed queue index. */
 #define TVBK_GROUP_SYNC_WORDS(groups) (2 + 2 * (groups))
 
-#define TVBK_RING_REGION_GUARD(ncvar) ((ncvar) == 1 ? 7 : 5)
+/* Region-major rings (launch.ring_layout = 1): slots per region -- the
+ * ring_len slots, then a guard of 6 (ncvar 2) or 10 (ncvar 1) slots mirroring
+ * slots 0, 1, ... (a four-step read loads one or two 32-byte chunks from the
+ * 32-byte boundary at or below its first slot, which may lie just below
+ * ring_len), rounded up so that every region starts on a 32-byte boundary.
+ * The ring itself must be 32-byte aligned. */
+#define TVBK_RING_REGION_GUARD(ncvar) ((ncvar) == 1 ? 10 : 6)
 #define TVBK_RING_REGION_STRIDE(ring_len, ncvar) \
-    ((((ring_len) + TVBK_RING_REGION_GUARD(ncvar)) + (4 / (ncvar)) - 1) / (4 / (ncvar)) * (4 / (ncvar)))
+    ((((ring_len) + TVBK_RING_REGION_GUARD(ncvar)) + (8 / (ncvar)) - 1) / (8 / (ncvar)) * (8 / (ncvar)))
 
 /* Smallest ring length (slots) usable with barrier interval sync_every. */
 int32_t tvbk_ring_len(int32_t horizon, int32_t sync_every);

@@ -85,6 +85,30 @@ def test_model_dims_and_ring_helpers():
     assert lib.tvbk_ring_smem_bytes(998, 2, 2001) == 0
 
 
+def test_header_layout_macros_match_the_binding(tmp_path):
+    """TVBK_RING_REGION_STRIDE / _GUARD and TVBK_GROUP_SYNC_WORDS, evaluated
+    by a C compiler from include/tvbk.h, equal the Python mirrors; regions of
+    region-major rings start on 32-byte boundaries."""
+    import shutil
+    import subprocess
+    cc = shutil.which('gcc') or shutil.which('cc')
+    if cc is None:
+        pytest.skip('no C compiler')
+    src = tmp_path / 'm.c'
+    src.write_text('#include <stdio.h>\n#include "tvbk.h"\nint main(void) {\n'
+                   '  for (int rl = 1; rl < 80; ++rl) for (int c = 1; c <= 2; ++c)\n'
+                   '    printf("%d %d %d %d\\n", rl, c, TVBK_RING_REGION_STRIDE(rl, c), TVBK_RING_REGION_GUARD(c));\n'
+                   '  printf("g %d\\n", TVBK_GROUP_SYNC_WORDS(9));\n  return 0;\n}\n')
+    exe = tmp_path / 'm'
+    subprocess.check_call([cc, '-std=c99', '-I', os.path.dirname(HEADER), str(src), '-o', str(exe)])
+    lines = subprocess.check_output([str(exe)], text=True).split('\n')
+    assert lines[-2] == 'g %d' % _lib.group_sync_words(9)
+    for ln in lines[:-2]:
+        rl, c, rs, guard = map(int, ln.split())
+        assert rs == _lib.ring_region_stride(rl, c)
+        assert rs >= rl + guard and (rs * c * 4) % 32 == 0
+
+
 def test_argument_errors_are_status_codes():
     lib = _lib.load()
     assert lib.tvbk_sim_run(None, None) == _lib.TVBK_ERR_INVALID

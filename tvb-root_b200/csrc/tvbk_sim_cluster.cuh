@@ -77,6 +77,25 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
     return t;
 }
 
+// 32-byte load through L2 (ld.global.cg.v8.f32, sm_100 and later); p is
+// 32-byte aligned.  The second form loads only when `on` and otherwise leaves
+// v as it was.
+__device__ __forceinline__ void ldcg32(const float* p, float (&v)[8]) {
+    asm volatile("ld.global.cg.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "l"(p)
+                 : "memory");
+}
+
+__device__ __forceinline__ void ldcg32_if(bool on, const float* p, float (&v)[8]) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %9, 0;\n\t"
+        "@q ld.global.cg.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t}"
+        : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7])
+        : "l"(p), "r"((int)on)
+        : "memory");
+}
+
 // Longest wait of one group barrier (all CTAs of a cooperative launch are
 // resident, so a wait this long means the launch cannot go on).
 constexpr uint64_t kGroupWaitNs = 4000000000ull;
@@ -538,12 +557,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 // runs are those of sim_kernel_cluster_runs, but the gather threads take four
 // steps at a time: for the next block of four steps an edge needs its
 // source's values at four consecutive times, which sit side by side in the
-// region-major ring -- one window of three (two for one coupling variable)
-// 16-byte L2 loads, the last only when the first time's slot is not on a
-// 16-byte boundary, instead of four scattered 8-byte loads, each of which
-// costs a 32-byte sector.  The window starts on a 16-byte boundary at or
-// below the first time's slot and may run past ring_len into the region's
-// guard slots, which mirror slots 0, 1, ....  The update warps advance the
+// region-major ring -- one or two 32-byte L2 loads (ld.global.cg.v8), the
+// second only when the four times cross a 32-byte boundary, instead of four
+// scattered 8-byte loads, each of which costs a 32-byte sector.  The window
+// starts on the 32-byte boundary at or below the first time's slot and may
+// run past ring_len into the region's guard slots, which mirror slots 0, 1,
+// ....  The update warps advance the
 // four steps of the current block from the partials gathered during the
 // previous block, so there is one CTA barrier per four steps.  The gather
 // of block b + 1 reads times up to 7 - d_min past the last time written
@@ -560,8 +579,7 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
     static_assert(CF == CF_LINEAR || CF == CF_DIFFERENCE, "blocked runs: Linear or Difference coupling");
     constexpr int NCV = M::NCV;
     constexpr int NG = NCV;
-    constexpr int SPC = 4 / NG;              // slots per 16-byte chunk
-    constexpr int NCH = NG == 2 ? 3 : 2;     // 16-byte chunks per four-step window
+    constexpr int SPW = 8 / NG;              // slots per 32-byte chunk
     extern __shared__ __align__(16) unsigned char sm[];
     tvbk_inst* __restrict__ Ip = L.insts + inst;
     int32_t* status = L.status + inst;
@@ -574,6 +592,11 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
     const int64_t s0 = Ip->step;
     const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
     if (s0 >= s_end) return true;  // uniform over the instance's CTAs
+    // the 32-byte window loads need a 32-byte aligned ring (uniform over the instance's CTAs)
+    if ((reinterpret_cast<uintptr_t>(Ip->ring) & 31) != 0) {
+        if (rank == 0 && threadIdx.x == 0) atomicOr(L.status + inst, TVBK_STATUS_UNSUPPORTED);
+        return true;
+    }
     const int nsteps = (int)(s_end - s0);
     const int tid = threadIdx.x;
     const int TB = blockDim.x;
@@ -662,7 +685,7 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
 #pragma unroll
         for (int k0 = 0; k0 < E; k0 += BE) {
             if (k0 < cnt) {
-                float4 win[BE][NCH];
+                float w0[BE][8], w1[BE][8];
                 int ov[BE];
                 float wv[BE];
 #pragma unroll
@@ -672,14 +695,15 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
                     const int d = ed.x >> 10, col = ed.x & 1023;
                     int sl = st0 - d;
                     sl += sl < 0 ? RL : 0;
-                    const int a = sl & ~(SPC - 1);
+                    const int a = sl & ~(SPW - 1);
                     ov[j] = sl - a;
                     wv[j] = __int_as_float(ed.y);
-                    const float4* src = reinterpret_cast<const float4*>(ring + ((size_t)col * RS + a) * NG);
+                    const float* src = ring + ((size_t)col * RS + a) * NG;
+                    ldcg32(src, w0[j]);
 #pragma unroll
-                    for (int c = 0; c < NCH; ++c)
-                        // the last chunk holds times only when the window starts below the first time's slot
-                        win[j][c] = (c < NCH - 1 || ov[j] != 0) ? __ldcg(src + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int c = 0; c < 8; ++c) w1[j][c] = 0.0f;
+                    // the next 32 bytes hold times only when the window starts in the chunk's last three slots
+                    ldcg32_if(ov[j] > SPW - 4, src + 8, w1[j]);
                 }
 #pragma unroll
                 for (int j = 0; j < BE; ++j) {
@@ -694,28 +718,40 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
                                     pa[r][q] = 0.0f;
                                 }
                         }
-                        float x[NCH * 4];
+                        float x[16];
 #pragma unroll
-                        for (int c = 0; c < NCH; ++c) {
-                            x[4 * c] = win[j][c].x;
-                            x[4 * c + 1] = win[j][c].y;
-                            x[4 * c + 2] = win[j][c].z;
-                            x[4 * c + 3] = win[j][c].w;
+                        for (int c = 0; c < 8; ++c) {
+                            x[c] = w0[j][c];
+                            x[8 + c] = w1[j][c];
                         }
+                        // the four times start o slots into the window: shift by o in binary steps
                         const int o = ov[j];
+                        float v[4][NG];
+                        if constexpr (NG == 2) {
+                            float y[10], z[8];
+#pragma unroll
+                            for (int c = 0; c < 10; ++c) y[c] = (o & 2) ? x[c + 4] : x[c];
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) z[c] = (o & 1) ? y[c + 2] : y[c];
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                v[r][0] = z[2 * r];
+                                v[r][NG - 1] = z[2 * r + 1];
+                            }
+                        } else {
+                            float y[7], z[5];
+#pragma unroll
+                            for (int c = 0; c < 7; ++c) y[c] = (o & 4) ? x[c + 4] : x[c];
+#pragma unroll
+                            for (int c = 0; c < 5; ++c) z[c] = (o & 2) ? y[c + 2] : y[c];
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) v[r][0] = (o & 1) ? z[r + 1] : z[r];
+                        }
                         const float w = wv[j];
 #pragma unroll
                         for (int r = 0; r < 4; ++r)
 #pragma unroll
-                            for (int q = 0; q < NG; ++q) {
-                                float v;
-                                if constexpr (NG == 2) {
-                                    v = o ? x[(r + 1) * 2 + q] : x[r * 2 + q];
-                                } else {
-                                    v = o == 0 ? x[r] : (o == 1 ? x[r + 1] : (o == 2 ? x[r + 2] : x[r + 3]));
-                                }
-                                pa[r][q] = fmaf(w, v, pa[r][q]);
-                            }
+                            for (int q = 0; q < NG; ++q) pa[r][q] = fmaf(w, v[r][q], pa[r][q]);
                     }
                 }
             }

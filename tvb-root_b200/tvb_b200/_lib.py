@@ -44,8 +44,8 @@ def group_sync_words(groups):
 
 def ring_region_stride(ring_len, ncvar):
     """Slots per region of a region-major ring (TVBK_RING_REGION_STRIDE)."""
-    spc = 4 // ncvar
-    return -(-(ring_len + (7 if ncvar == 1 else 5)) // spc) * spc
+    spc = 8 // ncvar
+    return -(-(ring_len + (10 if ncvar == 1 else 6)) // spc) * spc
 
 
 class Edge(ctypes.Structure):
