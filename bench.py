@@ -21,8 +21,10 @@ path); the time is the max over ranks.  At N = 1 the line also carries the
 Philox-path parity check against the oracle (Bold, state, FC), the serving
 leg (p50/p99 latency at a stated Poisson rate) and the large-network leg
 (region-steps/s and per-instance error against the float64 oracle).
-`--impl reference` times the CPU oracle (a numpy restatement of the
-reference's numpy path) on the host cores.
+`cpu_baseline` runs one instance per host core, spread over the (G, nsig)
+grid, for the full 60 s (600 000 steps).  `--impl reference` times the CPU
+oracle (a numpy restatement of the reference's numpy path) on the host
+cores, each step a shorter sample of the same kind (--ref-sample-steps).
 """
 import argparse
 import json
@@ -174,7 +176,7 @@ def _sample_text(cores, n_steps):
             'sample' % (cores, n_steps, n_steps * DT))
 
 
-def cpu_baseline(n_steps=20000, cores=None):
+def cpu_baseline(n_steps=600000, cores=None):
     import multiprocessing as mp
     cores = cores or os.cpu_count() or 1
     with mp.get_context('spawn').Pool(cores) as pool:
@@ -510,13 +512,14 @@ def run_reference(args, rank):
     with mp.get_context('spawn').Pool(cores) as pool:
         pool.map(_warm, range(cores))
         for k in range(args.warmup + args.steps):
-            wall, _ = cpu_sample(pool, cores, args.cpu_steps, offset=7 * k)
+            wall, _ = cpu_sample(pool, cores, args.ref_sample_steps, offset=7 * k)
             if k >= args.warmup:
                 walls.append(wall)
     t = float(np.mean(walls))
-    value = cores * args.cpu_steps * N_REGIONS / t
+    value = cores * args.ref_sample_steps * N_REGIONS / t
     full = 1024 * 600000 * N_REGIONS / value
-    cb = {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port', 'sample': _sample_text(cores, args.cpu_steps)}
+    cb = {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+          'sample': _sample_text(cores, args.ref_sample_steps)}
     line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 * t, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic', 'impl': 'reference',
@@ -538,7 +541,10 @@ def main():
     ap.add_argument('--instances', type=int, default=1024)
     ap.add_argument('--length', type=float, default=60000.0, help='simulated ms per instance')
     ap.add_argument('--chunk', type=int, default=None, help='steps per kernel launch')
-    ap.add_argument('--cpu-steps', type=int, default=20000)
+    ap.add_argument('--cpu-steps', type=int, default=600000,
+                    help='steps per instance of the cpu_baseline sample (default: the full 60 s)')
+    ap.add_argument('--ref-sample-steps', type=int, default=20000,
+                    help='steps per instance of each --impl reference sample (one sample per step)')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-steps', type=int, default=2)
     ap.add_argument('--gather', default='auto', choices=['auto', 'row', 'edge', 'split', 'tune'],
