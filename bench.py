@@ -406,9 +406,10 @@ def _epileptor_oracle_worker(args):
     from tvb_b200 import synthetic
     w, L = synthetic.connectome(EPI_N, 0.10, 5.0, 300.0, seed=4)
     kw = dict(history_dtype=np.float64) if variant == 'fp64' else {}
+    t0 = time.perf_counter()
     out, _ = O.simulate('Epileptor', {'x0': x0}, w, L, 3.0, EPI_DT, 'Difference', {'a': 0.1}, 'HeunDeterministic',
                         n_steps, [O.Monitor('TemporalAverage', 1.0)], buf0, st0, 0, **kw)
-    return k, variant, np.asarray(out[0][1])
+    return k, variant, np.asarray(out[0][1]), time.perf_counter() - t0
 
 
 def large_network_error(check_ms, cores):
@@ -423,11 +424,19 @@ def large_network_error(check_ms, cores):
     res = sw.run(fc=False)
     n_steps = sw.n_steps
     tasks = [(k, x0[k], n_steps, buf0, st0, v) for k in range(len(x0)) for v in ('stock', 'fp64')]
+    procs = min(cores, len(tasks))
     t0 = time.perf_counter()
-    with mp.get_context('spawn').Pool(min(cores, len(tasks))) as pool:
+    with mp.get_context('spawn').Pool(procs) as pool:
         outs = pool.map(_epileptor_oracle_worker, tasks)
     wall = time.perf_counter() - t0
-    ref = {(k, v): y for k, v, y in outs}
+    ref = {(k, v): y for k, v, y, _ in outs}
+    # the oracle's rate on these cores: each process runs its tasks one after another, every task the same
+    # number of steps (the stock task's rate is the reference's numpy path; the float64 one costs about the same)
+    t_task = float(np.mean([t for _, v, _, t in outs if v == 'stock']))
+    cpu = {'value': procs * n_steps * EPI_N / t_task, 'unit': UNIT, 'cores': procs, 'kind': 'port',
+           'sample': '%d processes, each an Epileptor 998 instance on the oracle (stock float32 history), %d steps '
+                     '(%g ms); value = processes x steps x regions / mean simulate time of one instance (the '
+                     'numpy path costs the same per step whatever the length)' % (procs, n_steps, check_ms)}
     windows = [m for m in range(20, int(check_ms) + 1, 20)]
     per = []
     for k in range(len(x0)):
@@ -443,7 +452,7 @@ def large_network_error(check_ms, cores):
              for v in ('vs_all_fp64', 'vs_stock')}
     return {'check_ms': check_ms, 'metric': 'max |device - oracle| / max |oracle| of TemporalAverage(1 ms) over '
             'the first t ms, from the same configured history', 'max_over_instances': worst, 'per_instance': per,
-            'nonfinite_instances': int((res['status'] != 0).sum()), 'oracle_wall_s': wall}
+            'nonfinite_instances': int((res['status'] != 0).sum()), 'oracle_wall_s': wall, 'cpu_baseline': cpu}
 
 
 def large_network_leg(steps, warmup, local, length_scale=1.0, gather='auto', cluster='auto', n_inst=16):
@@ -487,7 +496,9 @@ def run_large_network(args, rank, local):
                        'sync_every': leg['sync_every'], 'launch': leg['launch']},
             'nonfinite_instances': leg['nonfinite_instances'], 'gpu_launches': leg['gpu_launches']}
     if args.check_ms > 0:
-        line['error_vs_fp64_oracle'] = large_network_error(args.check_ms, os.cpu_count() or 1)
+        err = large_network_error(args.check_ms, os.cpu_count() or 1)
+        line['cpu_baseline'] = err.pop('cpu_baseline')
+        line['error_vs_fp64_oracle'] = err
     print(json.dumps(line), flush=True)
 
 
@@ -666,7 +677,9 @@ def main():
             serving = serving_leg(args.requests, args.rate, None, local, clocks=False)
             large = large_network_leg(1, 1, local)
             if args.check_ms > 0:
-                large['error_vs_fp64_oracle'] = large_network_error(args.check_ms, cores)
+                err = large_network_error(args.check_ms, cores)
+                large['cpu_baseline'] = err.pop('cpu_baseline')
+                large['error_vs_fp64_oracle'] = err
 
     if world > 1:
         tt = torch.tensor([t_dev, t_kern, float(np.median(e2e_times))], device='cuda', dtype=torch.float64)
