@@ -216,7 +216,9 @@ typedef struct tvbk_launch {
                                   * with more edges reads them from global memory (0: always global) */
     int32_t ring_layout;         /* 0: rings [ring_len][n][ncvar] (time-major).  1: region-major rings for the
                                   * cluster kernel's blocked edge runs (cluster > 1, edges_per_thread > 0,
-                                  * prefetch 1, Linear or Difference, ncvar 1 or 2, sync_every a multiple of 4
+                                  * prefetch 1, Linear, Difference or SigmoidalJansenRit (whose ring of
+                                  * pre-applied sigmoid values, one float per slot, is region-major too),
+                                  * ncvar 1 or 2, sync_every a multiple of 4
                                   * with 4 <= sync_every <= the smallest delay - 3): region r's times sit in
                                   * [r][TVBK_RING_REGION_STRIDE(ring_len, ncvar)][ncvar], time t in slot
                                   * t % ring_len, and the slots past ring_len mirror slots 0, 1, ... (every write

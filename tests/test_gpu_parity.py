@@ -463,10 +463,10 @@ def test_kernel_variants_agree(cfun):
         if not rr:
             assert sw.batch.ring_layout == 0
         out[key] = res
-    # time-major rings (one-step edge runs) always; region-major rings (four-step blocks) where the coupling
-    # gathers the model's own coupling variables, there also cooperative groups (all 8 instances at once)
-    assert layouts == ({0} if cfun == 'SigmoidalJansenRit' else {0, 1}), layouts
-    assert grouped == ({(0, 4)} if cfun == 'SigmoidalJansenRit' else {(8, 4)}), grouped
+    # time-major rings (one-step edge runs) and region-major rings (four-step blocks; for SigmoidalJansenRit a
+    # region-major ring of sigmoid values), there also cooperative groups (all 8 instances at once)
+    assert layouts == {0, 1}, layouts
+    assert grouped == {(8, 4)}, grouped
     bkey = [k for k in out if k[:6] == ('row', 1, None, 0, True, 'auto')][0]
     assert bkey[7] and bkey[8] == 0  # the row kernel with rings in shared memory
     base = out[bkey]

@@ -237,10 +237,12 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
                         "per row)");
         if (L->ring_layout == 1) {
             if (E == 0 || L->prefetch != 1 || d.ncvar > 2 ||
-                (L->cfun != TVBK_CFUN_LINEAR && L->cfun != TVBK_CFUN_DIFFERENCE) || L->sync_every < 4 ||
-                L->sync_every % 4 != 0 || L->max_n > 1024)
-                return fail(TVBK_ERR_INVALID, "tvbk_sim_run: region-major rings need edge runs, prefetch 1, Linear or "
-                            "Difference coupling, ncvar <= 2, sync_every a multiple of 4 and at most 1024 regions");
+                (L->cfun != TVBK_CFUN_LINEAR && L->cfun != TVBK_CFUN_DIFFERENCE &&
+                 L->cfun != TVBK_CFUN_SIGMOIDAL_JR) ||
+                L->sync_every < 4 || L->sync_every % 4 != 0 || L->max_n > 1024)
+                return fail(TVBK_ERR_INVALID, "tvbk_sim_run: region-major rings need edge runs, prefetch 1, Linear, "
+                            "Difference or SigmoidalJansenRit coupling, ncvar <= 2, sync_every a multiple of 4 and "
+                            "at most 1024 regions");
         }
         if (E == 0 && L->prefetch && L->cfun == TVBK_CFUN_DIFFERENCE)
             return fail(TVBK_ERR_INVALID, "tvbk_sim_run: a cluster with a warp per row cannot prefetch Difference "

@@ -576,9 +576,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 template <class M, int CF, int SCHEME, int E, bool EXT, class Sync>
 __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int inst, const int C, const int rank,
                                                  Sync& sync) {
-    static_assert(CF == CF_LINEAR || CF == CF_DIFFERENCE, "blocked runs: Linear or Difference coupling");
+    static_assert(CF == CF_LINEAR || CF == CF_DIFFERENCE || CF == CF_SIGMOIDAL_JR,
+                  "blocked runs: Linear, Difference or SigmoidalJansenRit coupling");
     constexpr int NCV = M::NCV;
-    constexpr int NG = NCV;
+    // SigmoidalJansenRit gathers a ring of pre-applied sigmoid values (one float per slot and region)
+    constexpr bool SIGMA = GatherTraits<CF, NCV>::SIGMA;
+    constexpr int NG = GatherTraits<CF, NCV>::NG;
     constexpr int SPW = 8 / NG;              // slots per 32-byte chunk
     extern __shared__ __align__(16) unsigned char sm[];
     tvbk_inst* __restrict__ Ip = L.insts + inst;
@@ -587,13 +590,16 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
     const int R = cluster_rows(n, C);
     const int r0 = min(n, rank * R), r1 = min(n, r0 + R), nr = r1 - r0;
     const int RL = Ip->ring_len;
-    const int RS = TVBK_RING_REGION_STRIDE(RL, NG);  // slots per region
+    const int RS = TVBK_RING_REGION_STRIDE(RL, NG);  // slots per region of the gathered ring
     constexpr int GUARD = TVBK_RING_REGION_GUARD(NG);
+    const int RSR = TVBK_RING_REGION_STRIDE(RL, NCV);  // of the state ring (the same one unless SIGMA)
+    constexpr int GUARDR = TVBK_RING_REGION_GUARD(NCV);
     const int64_t s0 = Ip->step;
     const int64_t s_end = min(Ip->step_end, s0 + L.max_steps);
     if (s0 >= s_end) return true;  // uniform over the instance's CTAs
     // the 32-byte window loads need a 32-byte aligned ring (uniform over the instance's CTAs)
-    if ((reinterpret_cast<uintptr_t>(Ip->ring) & 31) != 0) {
+    if (((reinterpret_cast<uintptr_t>(Ip->ring) | (SIGMA ? reinterpret_cast<uintptr_t>(Ip->pre_ring) : 0)) & 31) !=
+        0) {
         if (rank == 0 && threadIdx.x == 0) atomicOr(L.status + inst, TVBK_STATUS_UNSUPPORTED);
         return true;
     }
@@ -621,7 +627,7 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
     if (fits)
         for (int e = tid; e < ne; e += TB) {
             int2 r = __ldg(eg + e);
-            const int x = r.x / NCV;
+            const int x = r.x / NG;
             const int d = (x + n - 1) / n;
             r.x = d * 1024 + (d * n - x);
             esm[eslot(e)] = r;
@@ -637,8 +643,21 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
         if (Ip->aff != nullptr || (!EXT && (Ip->stim != nullptr || Ip->proj != nullptr)))
             atomicOr(status, TVBK_STATUS_UNSUPPORTED);
     }
-    float* __restrict__ ring = Ip->ring;
-    __syncthreads();
+    float* __restrict__ raw = Ip->ring;
+    float* __restrict__ ring = SIGMA ? Ip->pre_ring : raw;
+    if constexpr (SIGMA) {
+        // the sigmoid ring of this CTA's rows, guard slots included, from the state ring; every CTA's rows
+        // are ready after the barrier
+        for (int k = threadIdx.x; k < nr * (RL + GUARD); k += blockDim.x) {
+            const int lr = k / (RL + GUARD), t = k - lr * (RL + GUARD);
+            const float* v = raw + ((size_t)(r0 + lr) * RSR + (t < RL ? t : t - RL)) * NCV;
+            ring[(size_t)(r0 + lr) * RS + t] = sjr_pre(v[0], v[1], cf);
+        }
+        __syncthreads();
+        if (!sync()) return false;
+    } else {
+        __syncthreads();
+    }
 
     // this thread's run and the partials of row tid, as in sim_kernel_cluster_runs
     const int g = tid - T0;
@@ -783,9 +802,15 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
         post<CF, NCV>(a, cf, c);
         if (STOCH_BLOCK_START(ks)) node.noise_block(L, r0 + tid, s0 + 1 + ks);
         node.advance(L, Ip, r0 + tid, n, s0, ks, c);
-        float* dst = ring + ((size_t)(r0 + tid) * RS + wslot) * NCV;
+        float* dst = raw + ((size_t)(r0 + tid) * RSR + wslot) * NCV;
         node.write_ring(dst);
-        if (wslot < GUARD) node.write_ring(dst + (size_t)RL * NCV);  // the mirror past ring_len
+        if (wslot < GUARDR) node.write_ring(dst + (size_t)RL * NCV);  // the mirror past ring_len
+        if constexpr (SIGMA) {
+            const float pv = sjr_pre(node.x[M::cvar(0)], node.x[M::cvar(1)], cf);
+            float* pd = ring + (size_t)(r0 + tid) * RS + wslot;
+            pd[0] = pv;
+            if (wslot < GUARD) pd[RL] = pv;
+        }
     };
 
     const int K = L.sync_every;  // a multiple of 4
@@ -910,13 +935,14 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_group_blocks(co
 
 template <class M, int CF, int SCHEME, int E, bool EXT>
 int launch_cluster_blocks_t(const tvbk_launch& L, cudaStream_t st) {
-    if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE) {
+    if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE && CF != CF_SIGMOIDAL_JR) {
         return -2;
     } else {
         auto kern = sim_kernel_cluster_blocks<M, CF, SCHEME, E, EXT>;
         const int C = L.cluster;
         const int R = cluster_rows(L.max_n, C);
-        const size_t smem = cluster_blocks_head(R, M::NCV, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
+        constexpr int NG = GatherTraits<CF, M::NCV>::NG;
+        const size_t smem = cluster_blocks_head(R, NG, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
         if (smem > 227 * 1024) return -1;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
@@ -943,13 +969,14 @@ int launch_cluster_blocks_t(const tvbk_launch& L, cudaStream_t st) {
 
 template <class M, int CF, int SCHEME, int E, bool EXT>
 int launch_group_blocks_t(const tvbk_launch& L, cudaStream_t st) {
-    if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE) {
+    if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE && CF != CF_SIGMOIDAL_JR) {
         return -2;
     } else {
         auto kern = sim_kernel_group_blocks<M, CF, SCHEME, E, EXT>;
         const int C = L.cluster;
         const int R = cluster_rows(L.max_n, C);
-        const size_t smem = cluster_blocks_head(R, M::NCV, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
+        constexpr int NG = GatherTraits<CF, M::NCV>::NG;
+        const size_t smem = cluster_blocks_head(R, NG, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
         if (smem + 64 > 227 * 1024) return -1;  // 64: the kernel's own shared words
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;

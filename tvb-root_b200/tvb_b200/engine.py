@@ -347,8 +347,9 @@ class Batch:
                     self.sync_every = min(self.sync_every, dmin)
                 # blocked runs on region-major rings: four steps per gather, K a multiple of 4, <= d_min - 3
                 K4 = (min(self.sync_every, dmin - 3) // 4) * 4
-                if (region_rings and self.prefetch == 1 and K4 >= 4 and self.ncvar_gather == self.ncvar <= 2
-                        and self.cfun_id in (_lib.CFUN_IDS['Linear'], _lib.CFUN_IDS['Difference'])
+                if (region_rings and self.prefetch == 1 and K4 >= 4 and self.ncvar <= 2
+                        and self.cfun_id in (_lib.CFUN_IDS['Linear'], _lib.CFUN_IDS['Difference'],
+                                             _lib.CFUN_IDS['SigmoidalJansenRit'])
                         and self._cluster_smem(blocks=True) <= self.CLUSTER_SMEM):
                     self.ring_layout = 1
                     self.sync_every = K4
@@ -357,7 +358,7 @@ class Batch:
             self._choose_groups(groups, cluster, dmin)
         if self.cluster > 16 and not self.groups:
             raise ValueError('%d CTAs per instance need cooperative groups, which need region-major rings '
-                             '(Linear or Difference coupling, ncvar <= 2, smallest delay >= 7 steps)' % self.cluster)
+                             '(Linear, Difference or SigmoidalJansenRit coupling, ncvar <= 2, smallest delay >= 7 steps)' % self.cluster)
         self.slot_width, self._ring_len = self._choose_slots()
         self._plan()
         self.allocated = False
@@ -671,7 +672,8 @@ class Batch:
             if V > 1 and k % V == 0:
                 init.add(('ring', k), V * RL * n * self.ncvar * 4)
             if self.sigma and not self.ring_in_smem:
-                zero.add(('pre_ring', k), RL * n * 4)
+                # region-major rings: the sigmoid ring too, one float per slot (filled by the kernel)
+                zero.add(('pre_ring', k), (_lib.ring_region_stride(RL, 1) if self.ring_layout else RL) * n * 4)
             init.add(('state', k), self.nsv * n * 4)
             init.add(('params', k), max(self.nparam, 1) * n * 4)
             if s.stim is not None:
