@@ -97,3 +97,31 @@ def test_large_network_batches_plan_cooperative_groups():
     assert (b.groups, b.cluster) == (0, 16)
     b = plan(16, True, groups=4)
     assert b.groups == 4 and b.groups * b.cluster <= 148
+
+
+def test_sigmoidal_jansen_rit_plans_region_major_rings():
+    """JansenRit + SigmoidalJansenRit on 998 regions plans region-major rings
+    (a region-major ring of sigmoid values beside the state ring) and
+    cooperative groups; region_rings=False keeps time-major edge runs."""
+    from tvb_b200 import _lib, coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.engine import Batch
+    from tvb_b200.sweep import ParameterSweep
+    w, L = synthetic.connectome(998, 0.10, 5.0, 300.0, seed=2)
+
+    def plan(**kw):
+        sw = ParameterSweep(model=models.JansenRit(), connectivity=Connectivity(w, L, speed=3.0),
+                            coupling=coupling.SigmoidalJansenRit(), integrator=integrators.HeunDeterministic(dt=0.05),
+                            monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=10.0,
+                            sweep={'coupling.a': np.linspace(0.5, 2.0, 8)}, device='cpu').configure()
+        sim = sw._sim
+        return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, sw._noise_kind, sw.integrator.dt, sim._voi_codes,
+                     sw._specs, device='cpu', allocate=False, **kw)
+
+    b = plan()
+    assert b.sigma and b.ring_layout == 1 and b.groups == 8 and b.sync_every % 4 == 0
+    RL = b.meta[0]['ring_len']
+    assert b.zero.regions[('pre_ring', 0)][1] == _lib.ring_region_stride(RL, 1) * 998 * 4
+    b = plan(region_rings=False)
+    assert b.sigma and b.ring_layout == 0 and b.groups == 0 and b.edges_per_thread in (8, 16, 32)
+
