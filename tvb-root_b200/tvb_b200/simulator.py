@@ -364,6 +364,8 @@ class Simulator:
             self.log_nonfinite = True
         if st[0] & _lib.TVBK_STATUS_UNSUPPORTED:
             raise RuntimeError('the kernel variant chosen for this simulation does not write all its monitors')
+        if st[0] & _lib.TVBK_STATUS_TIMEOUT:
+            raise RuntimeError('a barrier of the cooperative launch gave up waiting: the run stopped early')
         out = batch.outputs_host()[0]
         if self._proj_istep:
             # the sensor projection of every sample: one float64 GEMM per monitor on the device

@@ -255,6 +255,8 @@ class ParameterSweep:
                 # instances of uneven lengths give a list of (T_i, nvoi, n) arrays
                 res[key] = np.stack(arrs) if len({a.shape for a in arrs}) == 1 else arrs
         res['status'] = self.batch.status()
+        if (res['status'] & _lib.TVBK_STATUS_TIMEOUT).any():
+            raise RuntimeError('a barrier of the cooperative launch gave up waiting: the run stopped early')
         res['instances'] = self.instances.copy()
         return res
 
