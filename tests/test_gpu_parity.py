@@ -494,6 +494,34 @@ def test_chunked_graph_replay_matches_one_launch():
     np.testing.assert_array_equal(outs['graph'], outs['one'])
 
 
+def test_group_launch_chunked_and_graph_replay_match_one_launch():
+    """The cooperative group launch (region-major rings, a device queue of
+    instances of uneven lengths) run as one launch, as eager chunks and as
+    chunks replayed from a CUDA graph gives bit-identical outputs."""
+    from tvb_b200 import coupling, integrators, models, monitors, synthetic
+    from tvb_b200.connectivity import Connectivity
+    from tvb_b200.sweep import ParameterSweep
+    w, L = synthetic.connectome(40, 0.4, 5.0, 60.0, seed=9)
+    outs = {}
+    for label, chunk, graph in (('one', None, False), ('eager', 96, False), ('graph', 96, True)):
+        np.random.seed(11)
+        sw = ParameterSweep(model=models.Epileptor(Ks=np.array([-0.2]), Kf=np.array([0.05])),
+                            connectivity=Connectivity(w, L, speed=5.0), coupling=coupling.Difference(),
+                            integrator=integrators.HeunDeterministic(dt=0.05),
+                            monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=40.0,
+                            sweep={'coupling.a': np.linspace(0.05, 0.2, 6),
+                                   'simulation_length': np.linspace(20.0, 40.0, 6)},
+                            ring_in_smem=False, cluster=4, groups=True, chunk_steps=chunk).configure()
+        sw.build()
+        assert sw.batch.groups == 6 and sw.batch.ring_layout == 1
+        sw.run_device(graph=graph)
+        outs[label] = [o['tavg'] for o in sw.batch.outputs_host()]
+        assert (sw.batch.status() == 0).all()
+    for a, b, c in zip(outs['one'], outs['eager'], outs['graph']):
+        np.testing.assert_array_equal(b, a)
+        np.testing.assert_array_equal(c, a)
+
+
 @pytest.mark.parametrize('case', ['scaling', 'sigmoidal', 'tanh', 'kuramoto', 'rk4'])
 def test_more_couplings_and_rk4_vs_reference(case):
     """Scaling, Sigmoidal, HyperbolicTangent, Kuramoto (coupling.py:203-322,489-508) and
