@@ -226,6 +226,10 @@ typedef struct tvbk_launch {
                                   * together, each edge reading its four consecutive times with 32-byte loads;
                                   * each instance's ring must be 32-byte aligned (else the instance is not
                                   * advanced and gets TVBK_STATUS_UNSUPPORTED) */
+    int32_t block_steps;         /* ring_layout 1: steps per gather block, 4 (or 0) or 8.  8 reads each edge's
+                                  * eight consecutive times at once (fewer scattered sector reads per step); it
+                                  * needs sync_every a multiple of 8 with 8 <= sync_every <= the smallest
+                                  * delay - 7, and launch.extras = 0 */
     int32_t groups;              /* 0: cluster > 1 launches one thread-block cluster per instance.  G > 0
                                   * (ring_layout 1 only): one cooperative launch of G x cluster CTAs, all
                                   * resident at once (at most the SMs' resident CTAs); each group of `cluster`
@@ -288,12 +292,12 @@ int tvbk_pack_edges(const int32_t* col, const int32_t* idelay, const float* weig
 #define TVBK_GROUP_SYNC_WORDS(groups) (2 + 2 * (groups))
 
 /* Region-major rings (launch.ring_layout = 1): slots per region -- the
- * ring_len slots, then a guard of 6 (ncvar 2) or 10 (ncvar 1) slots mirroring
- * slots 0, 1, ... (a four-step read loads one or two 32-byte chunks from the
+ * ring_len slots, then a guard of 10 (ncvar 2) or 14 (ncvar 1) slots mirroring
+ * slots 0, 1, ... (a block's read loads up to three 32-byte chunks from the
  * 32-byte boundary at or below its first slot, which may lie just below
  * ring_len), rounded up so that every region starts on a 32-byte boundary.
  * The ring itself must be 32-byte aligned. */
-#define TVBK_RING_REGION_GUARD(ncvar) ((ncvar) == 1 ? 10 : 6)
+#define TVBK_RING_REGION_GUARD(ncvar) ((ncvar) == 1 ? 14 : 10)
 #define TVBK_RING_REGION_STRIDE(ring_len, ncvar) \
     ((((ring_len) + TVBK_RING_REGION_GUARD(ncvar)) + (8 / (ncvar)) - 1) / (8 / (ncvar)) * (8 / (ncvar)))
 

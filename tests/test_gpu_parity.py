@@ -433,22 +433,26 @@ def test_kernel_variants_agree(cfun):
         sweep = {'coupling.a': np.linspace(0.5, 2.0, 8)}
         mons, length = [monitors.TemporalAverage(period=1.0)], 200.0
     out = {}
-    variants = [('row', 1, None, 0, True, 'auto'), ('row', 1, False, 0, True, 'auto'),
-                ('row', 'auto', None, 0, True, 'auto'), ('row', 1, False, 4, True, 'auto'),
-                ('row', 1, False, 16, True, 'auto'), ('row', 1, False, 16, False, 'auto'),
-                ('row', 1, False, 4, True, True), ('row', 1, False, 'auto', True, 'auto')]
+    variants = [('row', 1, None, 0, True, 'auto', 'auto'), ('row', 1, False, 0, True, 'auto', 'auto'),
+                ('row', 'auto', None, 0, True, 'auto', 'auto'), ('row', 1, False, 4, True, 'auto', 'auto'),
+                ('row', 1, False, 16, True, 'auto', 'auto'), ('row', 1, False, 16, False, 'auto', 'auto'),
+                ('row', 1, False, 16, True, 'auto', 4), ('row', 1, False, 4, True, True, 'auto'),
+                ('row', 1, False, 'auto', True, 'auto', 'auto')]
     if cfun != 'Difference':
-        variants += [('edge', 1, None, 0, True, 'auto'), ('split', 1, True, 0, True, 'auto')]
-    layouts, grouped = set(), set()
-    for gather, lanes, smem, cluster, rr, groups in variants:
+        variants += [('edge', 1, None, 0, True, 'auto', 'auto'), ('split', 1, True, 0, True, 'auto', 'auto')]
+    layouts, grouped, blocks = set(), set(), set()
+    for gather, lanes, smem, cluster, rr, groups, bsteps in variants:
         np.random.seed(11)
         sw = ParameterSweep(model=model, connectivity=Connectivity(w, L, speed=5.0), coupling=cf, integrator=integ(),
                             monitors=mons, simulation_length=length, sweep=sweep, gather=gather, lanes=lanes,
-                            ring_in_smem=smem, cluster=cluster, region_rings=rr, groups=groups).configure()
+                            ring_in_smem=smem, cluster=cluster, region_rings=rr, groups=groups,
+                            block_steps=bsteps).configure()
         res = sw.run(fc=False)
         assert (res['status'] == 0).all()
-        key = (gather, lanes, smem, cluster, rr, groups, sw.batch.lanes, sw.batch.ring_in_smem, sw.batch.cluster,
-               sw.batch.ring_layout, sw.batch.groups)
+        key = (gather, lanes, smem, cluster, rr, groups, bsteps, sw.batch.lanes, sw.batch.ring_in_smem,
+               sw.batch.cluster, sw.batch.ring_layout, sw.batch.groups)
+        if sw.batch.ring_layout:
+            blocks.add(sw.batch.block_steps)
         if lanes == 'auto':
             assert sw.batch.lanes == 8 // sw.batch.ncvar
         if gather == 'edge':
@@ -467,8 +471,9 @@ def test_kernel_variants_agree(cfun):
     # region-major ring of sigmoid values), there also cooperative groups (all 8 instances at once)
     assert layouts == {0, 1}, layouts
     assert grouped == {(8, 4)}, grouped
-    bkey = [k for k in out if k[:6] == ('row', 1, None, 0, True, 'auto')][0]
-    assert bkey[7] and bkey[8] == 0  # the row kernel with rings in shared memory
+    assert blocks == {4, 8}, blocks   # four- and eight-step blocks
+    bkey = [k for k in out if k[:7] == ('row', 1, None, 0, True, 'auto', 'auto')][0]
+    assert bkey[8] and bkey[9] == 0  # the row kernel with rings in shared memory
     base = out[bkey]
     for key, res in out.items():
         for mon in ('tavg', 'bold'):
@@ -494,16 +499,19 @@ def test_chunked_graph_replay_matches_one_launch():
     np.testing.assert_array_equal(outs['graph'], outs['one'])
 
 
-def test_group_launch_chunked_and_graph_replay_match_one_launch():
-    """The cooperative group launch (region-major rings, a device queue of
-    instances of uneven lengths) run as one launch, as eager chunks and as
-    chunks replayed from a CUDA graph gives bit-identical outputs."""
+@pytest.mark.parametrize('groups', [True, False])
+def test_group_launch_chunked_and_graph_replay_match_one_launch(groups):
+    """Blocked runs on region-major rings -- the cooperative group launch
+    (four-step blocks, a device queue of instances of uneven lengths) or
+    thread-block clusters (eight-step blocks) -- run as one launch, as eager
+    chunks of 100 steps (each ending inside a block) and as chunks replayed
+    from a CUDA graph give bit-identical outputs."""
     from tvb_b200 import coupling, integrators, models, monitors, synthetic
     from tvb_b200.connectivity import Connectivity
     from tvb_b200.sweep import ParameterSweep
     w, L = synthetic.connectome(40, 0.4, 5.0, 60.0, seed=9)
     outs = {}
-    for label, chunk, graph in (('one', None, False), ('eager', 96, False), ('graph', 96, True)):
+    for label, chunk, graph in (('one', None, False), ('eager', 100, False), ('graph', 100, True)):
         np.random.seed(11)
         sw = ParameterSweep(model=models.Epileptor(Ks=np.array([-0.2]), Kf=np.array([0.05])),
                             connectivity=Connectivity(w, L, speed=5.0), coupling=coupling.Difference(),
@@ -511,9 +519,10 @@ def test_group_launch_chunked_and_graph_replay_match_one_launch():
                             monitors=[monitors.TemporalAverage(period=1.0)], simulation_length=40.0,
                             sweep={'coupling.a': np.linspace(0.05, 0.2, 6),
                                    'simulation_length': np.linspace(20.0, 40.0, 6)},
-                            ring_in_smem=False, cluster=4, groups=True, chunk_steps=chunk).configure()
+                            ring_in_smem=False, cluster=4, groups=groups, chunk_steps=chunk).configure()
         sw.build()
-        assert sw.batch.groups == 6 and sw.batch.ring_layout == 1
+        assert sw.batch.ring_layout == 1
+        assert (sw.batch.groups, sw.batch.block_steps) == ((6, 4) if groups else (0, 8))
         sw.run_device(graph=graph)
         outs[label] = [o['tavg'] for o in sw.batch.outputs_host()]
         assert (sw.batch.status() == 0).all()

@@ -87,7 +87,14 @@ def test_large_network_batches_plan_cooperative_groups():
 
     b = plan(16, True)
     assert (b.ring_layout, b.groups, b.cluster) == (1, 9, 16) and b.edges_per_thread == 16
-    assert b.sync_every % 4 == 0 and 4 <= b.sync_every
+    # the group launch keeps four-step blocks (K a multiple of 4 with K <= d_min - 3), thread-block clusters
+    # take eight-step blocks (K a multiple of 8 with K <= d_min - 7)
+    dmin = min(sp.conn.min_delay for sp in b.specs)
+    assert b.block_steps == 4 and b.sync_every % 4 == 0 and 4 <= b.sync_every <= dmin - 3
+    b8 = plan(16, True, groups=False)
+    assert b8.block_steps == 8 and b8.sync_every % 8 == 0 and 8 <= b8.sync_every <= dmin - 7
+    b8 = plan(16, True, block_steps=8)
+    assert b8.groups == 9 and b8.block_steps == 8
     assert _lib.group_sync_words(b.groups) == 20
     b = plan(1, False)
     assert (b.groups, b.cluster) == (1, 64) and b.edges_per_thread in (8, 16, 32)

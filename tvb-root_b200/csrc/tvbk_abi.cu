@@ -220,6 +220,11 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
                     "one step at a time (prefetch 0, lanes 1, edges_per_thread 0, cluster 0)");
     if (L->ring_layout < 0 || L->ring_layout > 1 || (L->ring_layout == 1 && L->cluster <= 1))
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: ring_layout 1 (region-major) applies to clusters only");
+    if (L->block_steps != 0 && L->block_steps != 4 && L->block_steps != 8)
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: block_steps %d is not 0, 4 or 8", L->block_steps);
+    if (L->block_steps == 8 && (L->ring_layout != 1 || L->sync_every % 8 != 0 || L->extras != 0))
+        return fail(TVBK_ERR_INVALID, "tvbk_sim_run: block_steps 8 needs ring_layout 1, sync_every a multiple of 8 "
+                    "and extras 0");
     if (L->groups < 0 || (L->groups > 0 && (L->ring_layout != 1 || !L->group_sync)))
         return fail(TVBK_ERR_INVALID, "tvbk_sim_run: groups > 0 (cooperative launch) needs ring_layout 1 and "
                     "group_sync");
@@ -255,7 +260,8 @@ int tvbk_sim_run(const tvbk_launch* L, void* stream) {
         if (L->cluster_edges < 0) return fail(TVBK_ERR_INVALID, "tvbk_sim_run: cluster_edges < 0");
         const int64_t nacc = L->cfun == TVBK_CFUN_SIGMOIDAL_JR ? 1 : d.ncvar;
         // edge runs: row pointers, double-buffered partials of all 512 threads, the edges
-        const int64_t nbuf = L->ring_layout == 1 ? 4 : 1;  // blocked runs keep the partials of four steps
+        // blocked runs keep the partials of a block of steps
+        const int64_t nbuf = L->ring_layout == 1 ? (L->block_steps == 8 ? 8 : 4) : 1;
         const int64_t b = E ? ((R + 1) * 4 + 15) / 16 * 16 + (2 * nbuf * 512 * 2 * nacc * 4 + 15) / 16 * 16 +
                                   ((int64_t)L->cluster_edges + E) * 8
                             : ((R + 1) * 4 + 15) / 16 * 16 + (2 * R * nacc * 4 + 15) / 16 * 16 +

@@ -41,7 +41,7 @@ namespace cgx = cooperative_groups;
 
 constexpr int kClusterThreads = 512;
 constexpr int kClusterRowsPerPass = 4;
-// edges whose four-step windows a blocked-run gather thread requests together
+// edges whose four-step windows a blocked-run gather thread requests together (one for eight-step blocks)
 constexpr int kClusterBlockBatch = 2;
 // edges whose values an edge-run gather thread (one step per gather) requests together
 constexpr int kClusterRunBatch = 4;
@@ -128,9 +128,9 @@ __host__ __device__ inline size_t cluster_runs_head_rp(int R) { return ((size_t)
 __host__ __device__ inline size_t cluster_runs_head(int R, int ng, int threads) {
     return cluster_runs_head_rp(R) + ((size_t)2 * threads * 2 * ng * 4 + 15) / 16 * 16;
 }
-// the blocked variant keeps the partials of four steps: [2][4][2][ng][threads] floats
-__host__ __device__ inline size_t cluster_blocks_head(int R, int ng, int threads) {
-    return cluster_runs_head_rp(R) + ((size_t)2 * 4 * threads * 2 * ng * 4 + 15) / 16 * 16;
+// the blocked variant keeps the partials of a block of B steps: [2][B][2][ng][threads] floats
+__host__ __device__ inline size_t cluster_blocks_head(int R, int ng, int threads, int B) {
+    return cluster_runs_head_rp(R) + ((size_t)2 * B * threads * 2 * ng * 4 + 15) / 16 * 16;
 }
 
 // Shared memory of one cluster CTA: row pointers, the double-buffered sums
@@ -554,26 +554,27 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_runs(co
 }
 
 // Blocked edge runs on region-major rings (launch.ring_layout = 1).  The
-// runs are those of sim_kernel_cluster_runs, but the gather threads take four
-// steps at a time: for the next block of four steps an edge needs its
-// source's values at four consecutive times, which sit side by side in the
-// region-major ring -- one or two 32-byte L2 loads (ld.global.cg.v8), the
-// second only when the four times cross a 32-byte boundary, instead of four
-// scattered 8-byte loads, each of which costs a 32-byte sector.  The window
-// starts on the 32-byte boundary at or below the first time's slot and may
-// run past ring_len into the region's guard slots, which mirror slots 0, 1,
-// ....  The update warps advance the
-// four steps of the current block from the partials gathered during the
-// previous block, so there is one CTA barrier per four steps.  The gather
-// of block b + 1 reads times up to 7 - d_min past the last time written
-// before block b, so it needs d_min >= 7 and a cluster barrier interval
-// K <= d_min - 3, a multiple of 4 (the windows start on block boundaries).
+// runs are those of sim_kernel_cluster_runs, but the gather threads take a
+// block of B = 4 or 8 steps (launch.block_steps) at a time: for the next
+// block an edge needs its source's values at B consecutive times, which sit
+// side by side in the region-major ring -- one to three 32-byte L2 loads
+// (ld.global.cg.v8), the later ones only when the times reach into the next
+// 32-byte chunk, instead of B scattered 8-byte loads, each of which costs a
+// 32-byte sector.  The window starts on the 32-byte boundary at or below
+// the first time's slot and may run past ring_len into the region's guard
+// slots, which mirror slots 0, 1, ....  The update warps advance the steps
+// of the current block from the partials gathered during the previous
+// block, so there is one CTA barrier per block.  The gather of block b + 1
+// reads times up to 2B - 1 - d_min past the last time written before block
+// b, so it needs d_min >= 2B - 1 and a barrier interval K <= d_min - B + 1
+// between the instance's CTAs, a multiple of B (the windows start on block
+// boundaries).
 //
 // blocked_instance runs one instance's launch window on the C CTAs of the
 // instance (this CTA is `rank`); sync() is the barrier between those CTAs
 // (every K steps and at the end), which returns false when the launch is
 // being abandoned -- then so does blocked_instance.
-template <class M, int CF, int SCHEME, int E, bool EXT, class Sync>
+template <class M, int CF, int SCHEME, int E, bool EXT, int B, class Sync>
 __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int inst, const int C, const int rank,
                                                  Sync& sync) {
     static_assert(CF == CF_LINEAR || CF == CF_DIFFERENCE || CF == CF_SIGMOIDAL_JR,
@@ -612,7 +613,7 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
 
     int* rp = reinterpret_cast<int*>(sm);
     float* part = reinterpret_cast<float*>(sm + cluster_runs_head_rp(R));            // [2][4][2][NG][TB]
-    int2* esm = reinterpret_cast<int2*>(sm + cluster_blocks_head(R, NG, TB));       // the CTA's edges, interleaved
+    int2* esm = reinterpret_cast<int2*>(sm + cluster_blocks_head(R, NG, TB, B));    // the CTA's edges, interleaved
     const int e_lo = Ip->row_ptr[r0], e_hi = Ip->row_ptr[r1];
     const int ne = e_hi - e_lo;
     // as in sim_kernel_cluster_runs: a CTA whose edges do not fit flags the instance and only takes part in
@@ -688,23 +689,24 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
     }
 
     // partial (buffer pb, step r of the block, half h, variable q) of run u
-    auto pidx = [&](int pb, int r, int h, int q, int u) { return ((((pb * 4 + r) * 2 + h) * NG + q) * TB) + u; };
-    // couplings of the four steps after the time in slot st0: step r reads times (that time) + r - d.  The
+    auto pidx = [&](int pb, int r, int h, int q, int u) { return ((((pb * B + r) * 2 + h) * NG + q) * TB) + u; };
+    // couplings of the B steps after the time in slot st0: step r reads times (that time) + r - d.  The
     // edges go in batches of BE: the windows of a batch are all requested before the first is used, so a
     // thread waits for one L2 round trip per batch rather than one per edge.  Slots past the run's count
     // load a harmless in-bounds window (region 0 at st0) and add nothing.  One set of sums serves both
     // rows of a run: at the second row's first edge (kb) the first row's sums go to partial 0.
-    auto gather4 = [&](int st0, int pb) {
-        constexpr int BE = kClusterBlockBatch;
-        float pa[4][NG];
+    auto gatherB = [&](int st0, int pb) {
+        constexpr int BE = B == 4 ? kClusterBlockBatch : 1;
+        constexpr int NCH = (SPW - 1 + B + SPW - 1) / SPW;  // 32-byte chunks a window can touch
+        float pa[B][NG];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < B; ++r)
 #pragma unroll
             for (int q = 0; q < NG; ++q) pa[r][q] = 0.0f;
 #pragma unroll
         for (int k0 = 0; k0 < E; k0 += BE) {
             if (k0 < cnt) {
-                float w0[BE][8], w1[BE][8];
+                float wn[BE][NCH][8];
                 int ov[BE];
                 float wv[BE];
 #pragma unroll
@@ -718,11 +720,14 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
                     ov[j] = sl - a;
                     wv[j] = __int_as_float(ed.y);
                     const float* src = ring + ((size_t)col * RS + a) * NG;
-                    ldcg32(src, w0[j]);
+                    ldcg32(src, wn[j][0]);
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) w1[j][c] = 0.0f;
-                    // the next 32 bytes hold times only when the window starts in the chunk's last three slots
-                    ldcg32_if(ov[j] > SPW - 4, src + 8, w1[j]);
+                    for (int c = 1; c < NCH; ++c) {
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) wn[j][c][e] = 0.0f;
+                        // chunk c holds times of the window only when the window reaches past c chunks
+                        ldcg32_if(ov[j] + B > c * SPW, src + 8 * c, wn[j][c]);
+                    }
                 }
 #pragma unroll
                 for (int j = 0; j < BE; ++j) {
@@ -730,47 +735,32 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
                     if (k < cnt) {
                         if (k == kb) {
 #pragma unroll
-                            for (int r = 0; r < 4; ++r)
+                            for (int r = 0; r < B; ++r)
 #pragma unroll
                                 for (int q = 0; q < NG; ++q) {
                                     part[pidx(pb, r, 0, q, g)] = pa[r][q];
                                     pa[r][q] = 0.0f;
                                 }
                         }
-                        float x[16];
+                        float x[NCH * 8];
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            x[c] = w0[j][c];
-                            x[8 + c] = w1[j][c];
-                        }
-                        // the four times start o slots into the window: shift by o in binary steps
+                        for (int c = 0; c < NCH; ++c)
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) x[8 * c + e] = wn[j][c][e];
+                        // the B times start o slots into the window: shift by o one bit at a time, keeping
+                        // the floats still needed after each shift
                         const int o = ov[j];
-                        float v[4][NG];
-                        if constexpr (NG == 2) {
-                            float y[10], z[8];
 #pragma unroll
-                            for (int c = 0; c < 10; ++c) y[c] = (o & 2) ? x[c + 4] : x[c];
+                        for (int bit = SPW / 2; bit >= 1; bit /= 2) {
+                            const bool on = (o & bit) != 0;
 #pragma unroll
-                            for (int c = 0; c < 8; ++c) z[c] = (o & 1) ? y[c + 2] : y[c];
-#pragma unroll
-                            for (int r = 0; r < 4; ++r) {
-                                v[r][0] = z[2 * r];
-                                v[r][NG - 1] = z[2 * r + 1];
-                            }
-                        } else {
-                            float y[7], z[5];
-#pragma unroll
-                            for (int c = 0; c < 7; ++c) y[c] = (o & 4) ? x[c + 4] : x[c];
-#pragma unroll
-                            for (int c = 0; c < 5; ++c) z[c] = (o & 2) ? y[c + 2] : y[c];
-#pragma unroll
-                            for (int r = 0; r < 4; ++r) v[r][0] = (o & 1) ? z[r + 1] : z[r];
+                            for (int c = 0; c < (bit - 1 + B) * NG; ++c) x[c] = on ? x[c + bit * NG] : x[c];
                         }
                         const float w = wv[j];
 #pragma unroll
-                        for (int r = 0; r < 4; ++r)
+                        for (int r = 0; r < B; ++r)
 #pragma unroll
-                            for (int q = 0; q < NG; ++q) pa[r][q] = fmaf(w, v[r][q], pa[r][q]);
+                            for (int q = 0; q < NG; ++q) pa[r][q] = fmaf(w, x[r * NG + q], pa[r][q]);
                     }
                 }
             }
@@ -779,7 +769,7 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
         // never read), else partial 0
         const int h = kb < cnt ? 1 : 0;
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < B; ++r)
 #pragma unroll
             for (int q = 0; q < NG; ++q) part[pidx(pb, r, h, q, g)] = pa[r][q];
     };
@@ -815,9 +805,9 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
 
     const int K = L.sync_every;  // a multiple of 4
     const int bslot0 = (int)(s0 % RL);  // slot of the last time written before the first block
-    if (g >= 0) gather4(bslot0, 0);
+    if (g >= 0) gatherB(bslot0, 0);
     __syncthreads();
-    const int nblk = (nsteps + 3) >> 2;
+    const int nblk = (nsteps + B - 1) / B;
     // The two roles run separate loops, so that the model state is not held in the gather threads'
     // registers.  Both end every block with CTA barrier 1 over all threads and every K steps with sync(),
     // in the same order, and both see the same sync() results.
@@ -828,17 +818,17 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
             if (upd) {
                 int ws = bslot;
 #pragma unroll 1
-                for (int r = 0; r < 4; ++r) {
-                    const int ks = 4 * b + r;
+                for (int r = 0; r < B; ++r) {
+                    const int ks = B * b + r;
                     if (ks >= nsteps) break;
                     ws = (ws + 1 == RL) ? 0 : ws + 1;
                     update(ks, ws, b & 1, r);
                 }
             }
-            bslot += 4;
+            bslot += B;
             bslot -= bslot >= RL ? RL : 0;
             cta_barrier_all(TB);
-            since_sync += 4;
+            since_sync += B;
             if (since_sync >= K) {
                 since_sync = 0;
                 if (!sync()) {
@@ -852,14 +842,14 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
         int bslot = bslot0, since_sync = 0;
         for (int b = 0; b < nblk; ++b) {
             if (b + 1 < nblk) {
-                int nxt = bslot + 4;  // the next block's base time
+                int nxt = bslot + B;  // the next block's base time
                 nxt -= nxt >= RL ? RL : 0;
-                gather4(nxt, (b & 1) ^ 1);
+                gatherB(nxt, (b & 1) ^ 1);
             }
-            bslot += 4;
+            bslot += B;
             bslot -= bslot >= RL ? RL : 0;
             cta_barrier_all(TB);
-            since_sync += 4;
+            since_sync += B;
             if (since_sync >= K) {
                 since_sync = 0;
                 if (!sync()) {
@@ -876,7 +866,7 @@ __device__ __forceinline__ bool blocked_instance(const tvbk_launch& L, const int
 
 // One thread-block cluster of C CTAs per instance (cluster b takes instance
 // inst_order[b], or b); the cluster barrier keeps its CTAs in step.
-template <class M, int CF, int SCHEME, int E, bool EXT = true>
+template <class M, int CF, int SCHEME, int E, bool EXT, int B>
 __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(const tvbk_launch L) {
     cgx::cluster_group cluster = cgx::this_cluster();
     const int C = (int)cluster.num_blocks();
@@ -885,7 +875,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
         cluster_barrier();
         return true;
     };
-    blocked_instance<M, CF, SCHEME, E, EXT>(L, inst, C, (int)cluster.block_rank(), sync);
+    blocked_instance<M, CF, SCHEME, E, EXT, B>(L, inst, C, (int)cluster.block_rank(), sync);
 }
 
 // Cooperative form (launch.groups = G > 0): G x C CTAs, all resident at once.
@@ -897,7 +887,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_cluster_blocks(
 // SMs); groups fill every SM and take any C.  The group barrier is a counter
 // in global memory with a bounded wait; a barrier that gives up abandons the
 // launch, and every instance in flight gets TVBK_STATUS_TIMEOUT.
-template <class M, int CF, int SCHEME, int E, bool EXT = true>
+template <class M, int CF, int SCHEME, int E, bool EXT, int B>
 __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_group_blocks(const tvbk_launch L) {
     __shared__ int s_ok, s_next;
     const int C = L.cluster;
@@ -927,22 +917,22 @@ __global__ void __launch_bounds__(kClusterThreads, 1) sim_kernel_group_blocks(co
         const int j = s_next;
         if (j >= L.n_inst) return;
         inst = L.inst_order != nullptr ? L.inst_order[j] : j;
-        if (!blocked_instance<M, CF, SCHEME, E, EXT>(L, inst, C, rank, sync)) return;
+        if (!blocked_instance<M, CF, SCHEME, E, EXT, B>(L, inst, C, rank, sync)) return;
         // every CTA of the group has read the claim and is done with its shared memory before the next claim
         if (!sync()) return;
     }
 }
 
-template <class M, int CF, int SCHEME, int E, bool EXT>
+template <class M, int CF, int SCHEME, int E, bool EXT, int B>
 int launch_cluster_blocks_t(const tvbk_launch& L, cudaStream_t st) {
     if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE && CF != CF_SIGMOIDAL_JR) {
         return -2;
     } else {
-        auto kern = sim_kernel_cluster_blocks<M, CF, SCHEME, E, EXT>;
+        auto kern = sim_kernel_cluster_blocks<M, CF, SCHEME, E, EXT, B>;
         const int C = L.cluster;
         const int R = cluster_rows(L.max_n, C);
         constexpr int NG = GatherTraits<CF, M::NCV>::NG;
-        const size_t smem = cluster_blocks_head(R, NG, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
+        const size_t smem = cluster_blocks_head(R, NG, kClusterThreads, B) + ((size_t)L.cluster_edges + E) * 8;
         if (smem > 227 * 1024) return -1;
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
@@ -967,16 +957,16 @@ int launch_cluster_blocks_t(const tvbk_launch& L, cudaStream_t st) {
     }
 }
 
-template <class M, int CF, int SCHEME, int E, bool EXT>
+template <class M, int CF, int SCHEME, int E, bool EXT, int B>
 int launch_group_blocks_t(const tvbk_launch& L, cudaStream_t st) {
     if constexpr (CF != CF_LINEAR && CF != CF_DIFFERENCE && CF != CF_SIGMOIDAL_JR) {
         return -2;
     } else {
-        auto kern = sim_kernel_group_blocks<M, CF, SCHEME, E, EXT>;
+        auto kern = sim_kernel_group_blocks<M, CF, SCHEME, E, EXT, B>;
         const int C = L.cluster;
         const int R = cluster_rows(L.max_n, C);
         constexpr int NG = GatherTraits<CF, M::NCV>::NG;
-        const size_t smem = cluster_blocks_head(R, NG, kClusterThreads) + ((size_t)L.cluster_edges + E) * 8;
+        const size_t smem = cluster_blocks_head(R, NG, kClusterThreads, B) + ((size_t)L.cluster_edges + E) * 8;
         if (smem + 64 > 227 * 1024) return -1;  // 64: the kernel's own shared words
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
@@ -1002,22 +992,35 @@ int launch_group_blocks_t(const tvbk_launch& L, cudaStream_t st) {
     }
 }
 
-template <class M, int CF, int SCHEME, bool EXT>
-int launch_cluster_blocks(const tvbk_launch& L, cudaStream_t st) {
+template <class M, int CF, int SCHEME, bool EXT, int B>
+int launch_cluster_blocks_b(const tvbk_launch& L, cudaStream_t st) {
     if (L.groups > 0) {
         switch (L.edges_per_thread) {
-            case 8: return launch_group_blocks_t<M, CF, SCHEME, 8, EXT>(L, st);
-            case 16: return launch_group_blocks_t<M, CF, SCHEME, 16, EXT>(L, st);
-            case 32: return launch_group_blocks_t<M, CF, SCHEME, 32, EXT>(L, st);
+            case 8: return launch_group_blocks_t<M, CF, SCHEME, 8, EXT, B>(L, st);
+            case 16: return launch_group_blocks_t<M, CF, SCHEME, 16, EXT, B>(L, st);
+            case 32: return launch_group_blocks_t<M, CF, SCHEME, 32, EXT, B>(L, st);
             default: return -2;
         }
     }
     switch (L.edges_per_thread) {
-        case 8: return launch_cluster_blocks_t<M, CF, SCHEME, 8, EXT>(L, st);
-        case 16: return launch_cluster_blocks_t<M, CF, SCHEME, 16, EXT>(L, st);
-        case 32: return launch_cluster_blocks_t<M, CF, SCHEME, 32, EXT>(L, st);
+        case 8: return launch_cluster_blocks_t<M, CF, SCHEME, 8, EXT, B>(L, st);
+        case 16: return launch_cluster_blocks_t<M, CF, SCHEME, 16, EXT, B>(L, st);
+        case 32: return launch_cluster_blocks_t<M, CF, SCHEME, 32, EXT, B>(L, st);
         default: return -2;
     }
+}
+
+// Blocks of eight steps are built for the lean kernels (launch.extras = 0) only.
+template <class M, int CF, int SCHEME, bool EXT>
+int launch_cluster_blocks(const tvbk_launch& L, cudaStream_t st) {
+    if (L.block_steps == 8) {
+        if constexpr (EXT) {
+            return -2;
+        } else {
+            return launch_cluster_blocks_b<M, CF, SCHEME, EXT, 8>(L, st);
+        }
+    }
+    return launch_cluster_blocks_b<M, CF, SCHEME, EXT, 4>(L, st);
 }
 
 template <class M, int CF, int SCHEME, int E, bool PIPE, bool EXT>

@@ -45,7 +45,7 @@ def group_sync_words(groups):
 def ring_region_stride(ring_len, ncvar):
     """Slots per region of a region-major ring (TVBK_RING_REGION_STRIDE)."""
     spc = 8 // ncvar
-    return -(-(ring_len + (10 if ncvar == 1 else 6)) // spc) * spc
+    return -(-(ring_len + (14 if ncvar == 1 else 10)) // spc) * spc
 
 
 class Edge(ctypes.Structure):
@@ -130,6 +130,7 @@ class Launch(ctypes.Structure):
         ('cluster', ctypes.c_int32),
         ('cluster_edges', ctypes.c_int32),
         ('ring_layout', ctypes.c_int32),
+        ('block_steps', ctypes.c_int32),
         ('groups', ctypes.c_int32),
         ('group_sync', ctypes.c_void_p),
         ('extras', ctypes.c_int32),

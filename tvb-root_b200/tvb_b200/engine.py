@@ -253,7 +253,7 @@ class InstanceSpec:
 class Batch:
     def __init__(self, model_id, cfun_id, scheme_id, noise_kind, dt, voi_codes, specs, device=None,
                  sync_every=None, ring_in_smem=None, gather='auto', lanes=1, allocate=True, cluster='auto',
-                 region_rings=True, groups='auto'):
+                 region_rings=True, groups='auto', block_steps='auto'):
         self.lib = _lib.load()
         self.device = torch.device(device if device is not None else 'cuda')
         self.model_id, self.cfun_id, self.scheme_id, self.noise_kind = model_id, cfun_id, scheme_id, noise_kind
@@ -337,6 +337,7 @@ class Batch:
         self._cluster_max = 256 if (groups is not False and groups not in (0, None, 'off', 'auto')) else 16
         self.cluster, self.cluster_edges = self._choose_cluster(cluster)
         self.ring_layout = 0
+        self.block_steps = 0
         if self.cluster:
             # edge runs for the cluster CTAs when they fit; with them Difference also prefetches
             runs = self._choose_cluster_runs(dmin)
@@ -345,17 +346,30 @@ class Batch:
                 if dmin >= 1 and self.cfun_id == _lib.CFUN_IDS['Difference']:
                     self.prefetch = 1
                     self.sync_every = min(self.sync_every, dmin)
-                # blocked runs on region-major rings: four steps per gather, K a multiple of 4, <= d_min - 3
-                K4 = (min(self.sync_every, dmin - 3) // 4) * 4
+                # blocked runs on region-major rings: B = 4 or 8 steps per gather, K a multiple of B with
+                # K <= d_min - B + 1 (d_min >= 2B - 1); eight-step blocks for the lean kernel only
+                K0 = self.sync_every
+                K4 = (min(K0, dmin - 3) // 4) * 4
+                K8 = (min(K0, dmin - 7) // 8) * 8
                 if (region_rings and self.prefetch == 1 and K4 >= 4 and self.ncvar <= 2
                         and self.cfun_id in (_lib.CFUN_IDS['Linear'], _lib.CFUN_IDS['Difference'],
                                              _lib.CFUN_IDS['SigmoidalJansenRit'])
-                        and self._cluster_smem(blocks=True) <= self.CLUSTER_SMEM):
+                        and self._cluster_smem(blocks=4) <= self.CLUSTER_SMEM):
                     self.ring_layout = 1
-                    self.sync_every = K4
+                    self.block_steps, self.sync_every = 4, K4
+                    if (block_steps in ('auto', 8) and K8 >= 8 and self.extras == 0
+                            and self._cluster_smem(blocks=8) <= self.CLUSTER_SMEM):
+                        self.block_steps, self.sync_every = 8, K8
+                    elif block_steps == 8:
+                        raise ValueError('eight-step blocks need a smallest delay of 15 steps, no stimulus, '
+                                         'AfferentCoupling or projection stream, and the partials in shared memory')
         self.groups = 0
         if self.ring_layout == 1:
             self._choose_groups(groups, cluster, dmin)
+            if self.groups and block_steps == 'auto' and self.block_steps == 8:
+                # measured: eight-step blocks gain on thread-block clusters (+18 % on the large-network batch)
+                # but not under the group launch (-2 %), whose barrier interval they shorten
+                self.block_steps, self.sync_every = 4, K4
         if self.cluster > 16 and not self.groups:
             raise ValueError('%d CTAs per instance need cooperative groups, which need region-major rings '
                              '(Linear, Difference or SigmoidalJansenRit coupling, ncvar <= 2, smallest delay >= 7 steps)' % self.cluster)
@@ -546,7 +560,7 @@ class Batch:
             self.cluster, self.cluster_edges = C, edges
             runs = self._choose_cluster_runs(dmin)
             self.edges_per_thread = runs
-            fits = runs and self._cluster_smem(blocks=True) + 64 <= self.CLUSTER_SMEM
+            fits = runs and self._cluster_smem(blocks=self.block_steps) + 64 <= self.CLUSTER_SMEM
             self.cluster, self.cluster_edges, self.edges_per_thread = keep
             if not fits:
                 continue
@@ -558,13 +572,13 @@ class Batch:
         _, C, G, edges, runs = best
         self.cluster, self.cluster_edges, self.edges_per_thread, self.groups = C, edges, runs, G
 
-    def _cluster_smem(self, blocks=False):
+    def _cluster_smem(self, blocks=0):
         """Shared memory of an edge-run cluster CTA: row pointers, the
-        double-buffered partials (of four steps for the blocked runs) and the
-        CTA's edges with room for the interleaving."""
+        double-buffered partials (of a block of `blocks` steps for the blocked
+        runs) and the CTA's edges with room for the interleaving."""
         R = -(-self.max_n // self.cluster)
         nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
-        parts = 2 * (4 if blocks else 1) * self.CLUSTER_THREADS * 2 * nacc * 4
+        parts = 2 * max(int(blocks), 1) * self.CLUSTER_THREADS * 2 * nacc * 4
         return -(-(R + 1) * 4 // 16) * 16 + -(-parts // 16) * 16 + 8 * (self.cluster_edges + max(self.CLUSTER_RUNS))
 
     def _choose_cluster_runs(self, dmin):
@@ -953,6 +967,7 @@ class Batch:
         L.cluster = self.cluster
         L.cluster_edges = self.cluster_edges
         L.ring_layout = self.ring_layout
+        L.block_steps = self.block_steps
         L.groups = self.groups
         L.group_sync = self._group_sync.data_ptr() if self.groups else None
         L.extras = self.extras

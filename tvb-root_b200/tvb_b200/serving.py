@@ -138,7 +138,7 @@ class SimulationServer:
         # launch reads
         key = (sim._model_id, sim._cfun_id, sim._scheme_id, noise_kind, float(np.float32(sim.integrator.dt)),
                tuple(sim._voi_codes), sim.number_of_nodes, plan.ring_in_smem, plan.cluster, plan.prefetch,
-               plan.sigma, plan.edges_per_thread if plan.cluster else 0, plan.ring_layout)
+               plan.sigma, plan.edges_per_thread if plan.cluster else 0, plan.ring_layout, plan.block_steps)
         req = _Request(rid, sim, spec, noise_kind, key, plan, time.perf_counter() if t_submit is None else t_submit)
         if req.footprint > self.budget:
             raise ValueError('request needs %d bytes, more than the budget of %d' % (req.footprint, self.budget))
@@ -215,7 +215,8 @@ class SimulationServer:
         L.cluster = p0.cluster
         L.cluster_edges = max(p.cluster_edges for p in plans)
         L.edges_per_thread = p0.edges_per_thread if p0.cluster else 0   # edge runs (one value per group)
-        L.ring_layout = p0.ring_layout   # one value per group; region-major rings keep sync_every a multiple of 4
+        # one value per group; region-major rings keep sync_every a multiple of the block length
+        L.ring_layout, L.block_steps = p0.ring_layout, p0.block_steps
         L.extras = 0
         for p in plans:
             L.extras |= p.extras

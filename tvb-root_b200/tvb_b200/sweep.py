@@ -52,13 +52,16 @@ class ParameterSweep:
     groups: with region-major rings, 'auto' (and cluster='auto') runs the
     batch as one cooperative launch of groups of CTAs that take instances
     from a device queue, choosing the CTAs per instance; True also with an
-    explicit cluster; False keeps thread-block clusters.
+    explicit cluster; False keeps thread-block clusters.  block_steps: steps
+    per gather block on region-major rings, 4, 8 or 'auto' (8 when the
+    smallest delay allows and the batch has no stimulus, AfferentCoupling or
+    projection stream).
     """
 
     def __init__(self, model, connectivity, coupling, integrator, monitors, simulation_length, sweep,
                  noise_source='philox', chunk_steps=None, device=None, sync_every=None, ring_in_smem=None,
                  gather='auto', lanes=1, cluster='auto', stimulus=None, shard=None, instances=None,
-                 region_rings=True, groups='auto'):
+                 region_rings=True, groups='auto', block_steps='auto'):
         self.model = adopt_model(model)
         self.stimulus = stimulus
         self.connectivity = adopt_connectivity(connectivity)
@@ -85,6 +88,7 @@ class ParameterSweep:
         self.cluster = cluster
         self.region_rings = region_rings
         self.groups = groups
+        self.block_steps = block_steps
         self.batch = None
 
     def configure(self):
@@ -162,7 +166,7 @@ class ParameterSweep:
         return Batch(sim._model_id, sim._cfun_id, sim._scheme_id, self._noise_kind, self.integrator.dt,
                      sim._voi_codes, self._specs, device=self.device, sync_every=self.sync_every,
                      ring_in_smem=ring_in_smem, gather=gather, lanes=lanes, cluster=cluster,
-                     region_rings=self.region_rings, groups=self.groups)
+                     region_rings=self.region_rings, groups=self.groups, block_steps=self.block_steps)
 
     def projection(self, mons):
         """Sensor signals of projection monitors `mons` for all instances: one
