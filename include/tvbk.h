@@ -222,8 +222,9 @@ typedef struct tvbk_launch {
                                   * with 4 <= sync_every <= the smallest delay - 3): region r's times sit in
                                   * [r][TVBK_RING_REGION_STRIDE(ring_len, ncvar)][ncvar], time t in slot
                                   * t % ring_len, and the slots past ring_len mirror slots 0, 1, ... (every write
-                                  * of a mirrored slot also writes its mirror).  Four steps' couplings are gathered
-                                  * together, each edge reading its four consecutive times with 32-byte loads;
+                                  * of a mirrored slot also writes its mirror).  A block of block_steps steps'
+                                  * couplings is gathered together, each edge reading its consecutive times with
+                                  * 32-byte loads;
                                   * each instance's ring must be 32-byte aligned (else the instance is not
                                   * advanced and gets TVBK_STATUS_UNSUPPORTED) */
     int32_t block_steps;         /* ring_layout 1: steps per gather block, 4 (or 0) or 8.  8 reads each edge's
