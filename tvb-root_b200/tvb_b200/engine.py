@@ -265,14 +265,16 @@ class Batch:
         if not self.specs:
             raise ValueError('empty batch')
         # barrier interval: no read of a time written inside a window (K <= d_min + 1)
-        dmin = min(s.conn.min_delay for s in self.specs)
+        # the distinct connectomes (a sweep shares one): the planning below depends on them only
+        self._uconns = list({id(s.conn): s.conn for s in self.specs}.values())
+        dmin = min(c.min_delay for c in self._uconns)
         K = dmin + 1 if sync_every is None else int(sync_every)
         K = max(1, min(K, dmin + 1))
-        self.max_n = max(s.conn.n for s in self.specs)
-        self.max_degree = max(int(np.diff(s.conn.row_ptr).max()) if s.conn.nnz else 0 for s in self.specs)
+        self.max_n = max(c.n for c in self._uconns)
+        self.max_degree = max(int(np.diff(c.row_ptr).max()) if c.nnz else 0 for c in self._uconns)
         if self.max_n > _lib.MAX_REGIONS:
             raise ValueError('%d regions exceed this build (%d)' % (self.max_n, _lib.MAX_REGIONS))
-        hmax = max(s.conn.horizon for s in self.specs)
+        hmax = max(c.horizon for c in self._uconns)
         # AfferentCoupling is written by the row kernel only
         self.afferent = any(s.aff_istep for s in self.specs)
         # launch.extras: without a stimulus or AfferentCoupling the row kernel runs its lean build
@@ -454,7 +456,7 @@ class Batch:
         (occ, K) = max((ctas(padded(K)), K) for K in cands)
         if occ == 0 or occ < ctas(plain(K0)):
             return 0, plain(K0)
-        if any(s.conn.slot_table(width) is None for s in self.specs):
+        if any(c.slot_table(width) is None for c in self._uconns):
             return 0, plain(K0)
         self.sync_every = K
         return width, padded(K)
@@ -493,14 +495,7 @@ class Batch:
         R = -(-self.max_n // C)
         nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
         head = -(-(R + 1) * 4 // 16) * 16 + -(-2 * R * nacc * 4 // 16) * 16
-        emax = 0
-        for s in self.specs:
-            rp = s.conn.row_ptr
-            n = s.conn.n
-            for r in range(C):
-                lo = min(n, r * R)
-                hi = min(n, lo + R)
-                emax = max(emax, int(rp[hi] - rp[lo]))
+        emax = self._cluster_edges_for(C)
         return C, (emax if head + 8 * emax <= self.CLUSTER_SMEM else 0)
 
     CLUSTER_THREADS = 512
@@ -516,9 +511,9 @@ class Batch:
         """Largest edge count of one CTA's rows with C CTAs per instance."""
         R = -(-self.max_n // C)
         emax = 0
-        for s in self.specs:
-            rp = s.conn.row_ptr
-            n = s.conn.n
+        for c in self._uconns:
+            rp = c.row_ptr
+            n = c.n
             for r in range(C):
                 lo = min(n, r * R)
                 hi = min(n, lo + R)
@@ -597,10 +592,10 @@ class Batch:
             return 0
         ahead = dmin >= 1 and self.model_id != _lib.MODEL_IDS['Sum']
         need, cap = 1, 1 << 30
-        for s in self.specs:
-            rp = np.asarray(s.conn.row_ptr)
+        for c in self._uconns:
+            rp = np.asarray(c.row_ptr)
             deg = np.diff(rp)
-            n = s.conn.n
+            n = c.n
             for r in range(C):
                 lo, hi = min(n, r * R), min(n, r * R + R)
                 nr = hi - lo
@@ -629,8 +624,7 @@ class Batch:
         K = 2 if dmin >= 1 else 1
         nacc = 1 if self.cfun_id == _lib.CFUN_IDS['SigmoidalJansenRit'] else self.ncvar
         need = []
-        for s in self.specs:
-            c = s.conn
+        for c in self._uconns:
             if c.nnz == 0:
                 return None
             deg = np.diff(c.row_ptr)
