@@ -50,11 +50,27 @@ def _compile(src, force, verbose, extra):
     return obj, (r.stderr if verbose else None)
 
 
+# Relative compile times of the simulation translation units (model x scheme), so that the longest start
+# first and the parallel build does not end on one long unit.
+_MODEL_COST = {'jr': 4, 'epileptor': 3, 'rww': 2, 'g2d': 2, 'sum': 1}
+_SCHEME_COST = {'heun_stoch': 4, 'rk4': 4, 'heun_det': 3, 'euler_stoch': 2, 'euler_det': 1}
+
+
+def _compile_cost(src):
+    name = os.path.basename(src)[:-3]
+    if not name.startswith('tvbk_sim_'):
+        return (0, name)
+    parts = name[len('tvbk_sim_'):]
+    model = parts.split('_')[0]
+    scheme = parts[len(model) + 1:]
+    return (_MODEL_COST.get(model, 1) * _SCHEME_COST.get(scheme, 1), name)
+
+
 def build(force=False, verbose=False, extra=()):
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, '*.cu')))
-    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+    srcs = sorted(glob.glob(os.path.join(CSRC, '*.cu')), key=_compile_cost, reverse=True)
+    with cf.ThreadPoolExecutor(max_workers=min(max(os.cpu_count() or 1, 1), 16, len(srcs))) as ex:
         results = list(ex.map(lambda s: _compile(s, force, verbose, list(extra)), srcs))
     objs = [o for o, _ in results]
     for _, log in results:
